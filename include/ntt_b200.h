@@ -1,0 +1,153 @@
+/*
+ * ntt_b200.h - C ABI of the B200 (sm_100a) CKKS NTT / ModUp / ModDown / Hybrid
+ * key-switch path.
+ *
+ * The reference (minnow54426/ntt-gpu) reaches its CUDA path through the C++
+ * transport seam ntt::resident::detail::Driver (include/ntt/resident_driver.hpp:13-57)
+ * created by make_cuda_session (include/ntt/resident.hpp:142-143). Each entry
+ * point below replaces one Driver primitive or one Session composite; the
+ * replaced interface is named in the comment. The C++ Driver in
+ * ntt_gpu_b200/host maps these status codes onto the reference's exceptions.
+ *
+ * Conventions
+ *  - Towers are addressed by global id: Q tower i -> i, P tower j -> M + j.
+ *  - Polynomials are limb-major u64 arrays: tower t occupies words [t*N, t*N+N).
+ *    Coefficient form is natural order; evaluation form is the bit-reversed
+ *    order of the reference (evaluation at psi^(2j+1), include/ntt/ntt.hpp:5-35).
+ *  - All residues are canonical u64 in [0, q). Inputs must be canonical.
+ *  - Pointers named dst/src/... are device pointers on the context's device.
+ *    `stream` is a cudaStream_t (NULL = legacy default stream). Work is only
+ *    enqueued; callers synchronise on the stream.
+ *  - Every call validates its arguments on the host and returns a contract
+ *    error BEFORE anything is enqueued (reference: ContractError thrown before
+ *    enqueue, include/ntt/backend_contract.hpp:20-26).
+ *  - Scratch: composite operations take a caller-provided device workspace whose
+ *    size ntt_b200_workspace_bytes reports; they never allocate.
+ */
+#ifndef NTT_B200_H
+#define NTT_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define NTT_B200_OK 0
+#define NTT_B200_ERR_CONTRACT 1    /* invalid argument / layout (reference ContractError) */
+#define NTT_B200_ERR_CUDA 2        /* CUDA runtime failure ("CUDA: <call>: <msg>") */
+#define NTT_B200_ERR_UNSUPPORTED 3 /* valid input outside this build's capability */
+#define NTT_B200_ERR_WORKSPACE 4   /* workspace missing or too small */
+#define NTT_B200_ERR_TIMEOUT 5     /* a bounded device wait expired */
+
+typedef struct ntt_b200_context_s *ntt_b200_context;
+
+/* Message of the last failing call on this host thread. */
+const char *ntt_b200_last_error(void);
+/* Number of this library's kernels launched by this process so far. */
+uint64_t ntt_b200_kernel_launches(void);
+
+/* Build a context: validates parameters as proposal::Parameters::create does
+ * (include/ntt/backend_contract.hpp:48-66), builds twiddle, conversion and
+ * correction tables and keeps them resident in HBM. Replaces the table setup
+ * of the reference's CUDA Context (src/cuda/resident_adapter.inc:60-103) and
+ * make_cuda_session (src/cuda/resident_adapter.inc:306-317). k may be 0 for a
+ * transform-only context; alpha is the full-context digit width
+ * (OpenFHE GetNumPerPartQ). */
+int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n,
+                            const uint64_t *q, const uint64_t *q_psi, size_t m,
+                            const uint64_t *p, const uint64_t *p_psi, size_t k,
+                            size_t alpha);
+int ntt_b200_context_destroy(ntt_b200_context ctx);
+/* Bytes of device tables the context holds (Driver::constant_bytes,
+ * include/ntt/resident_driver.hpp:28). */
+int ntt_b200_context_table_bytes(ntt_b200_context ctx, size_t *out);
+/* Build every conversion/correction plan a key switch at `level` needs, so that
+ * later calls at that level perform no host work or table upload. */
+int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level);
+
+/* Forward (inverse = 0) or inverse NTT of `polys` polynomials. Slot i of poly p
+ * is read at src + p*poly_stride + i*N and written at dst + p*poly_stride + i*N
+ * (dst may equal src) with the tables of tower_ids[i]. Replaces
+ * Driver::transform (include/ntt/resident_driver.hpp:34; src/cuda/ntt_kernels.cu:286-326). */
+int ntt_b200_ntt(ntt_b200_context ctx, uint64_t *dst, const uint64_t *src,
+                 const uint32_t *tower_ids, size_t towers, size_t polys,
+                 size_t poly_stride, int inverse, void *stream);
+
+/* dst = left * right pointwise (evaluation form). Replaces Driver::pointwise
+ * (include/ntt/resident_driver.hpp:35-36). */
+int ntt_b200_pointwise(ntt_b200_context ctx, uint64_t *dst, const uint64_t *left,
+                       const uint64_t *right, const uint32_t *tower_ids, size_t towers,
+                       size_t polys, size_t poly_stride, void *stream);
+
+/* Coefficient-domain approximate CRT switch (unreduced lift) from the source
+ * towers (contiguous at src) to the target towers (contiguous at dst).
+ * Replaces Driver::switch_basis (include/ntt/resident_driver.hpp:45-47;
+ * include/ntt/basis_conversion.hpp:13-30). Sources and targets: 1..40, disjoint. */
+int ntt_b200_switch_basis(ntt_b200_context ctx, uint64_t *dst, const uint64_t *src,
+                          const uint32_t *source_ids, size_t s, const uint32_t *target_ids,
+                          size_t t, void *stream);
+
+/* ModDown tail on the active Q towers: dst = (left - right) * [P^-1]_q.
+ * Replaces Driver::correct (include/ntt/resident_driver.hpp:48-50;
+ * include/ntt/resident_conversion.hpp:45-49). */
+int ntt_b200_correct(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *left,
+                     const uint64_t *right, void *stream);
+
+/* Hybrid MAC over all active digits in one pass:
+ *   out_b = sum_d digits[d] * key_b[d][row],  out_a likewise,
+ * digits: beta x (L+K) towers (evaluation QP); keys: FULL-context digits of
+ * (M+K) towers each, rows selected by key_indices (i for Q, M+j for P).
+ * Replaces the per-digit Driver::hybrid_mac loop (include/ntt/resident_driver.hpp:37-40;
+ * src/resident.cpp:530-570) and Session::upload_hybrid_key's row packing
+ * (src/resident.cpp:492-529). */
+int ntt_b200_hybrid_mac(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                        const uint64_t *digits, const uint64_t *key_b, const uint64_t *key_a,
+                        void *stream);
+
+/* out = automorphism(ext) with P*c0 added on the Q towers of the b channel.
+ * automorphism must be odd and < 2N. Replaces Driver::hybrid_rotate
+ * (include/ntt/resident_driver.hpp:41-44; src/resident.cpp:571-617). */
+int ntt_b200_hybrid_rotate(ntt_b200_context ctx, size_t level, uint64_t *out_b,
+                           uint64_t *out_a, const uint64_t *ext_b, const uint64_t *ext_a,
+                           const uint64_t *c0, uint32_t automorphism, void *stream);
+
+/* Workspace sizes (bytes) of the composite operations below. */
+#define NTT_B200_OP_MOD_UP 1
+#define NTT_B200_OP_MOD_DOWN 2
+#define NTT_B200_OP_DIGITS 3
+#define NTT_B200_OP_KEYSWITCH 4
+int ntt_b200_workspace_bytes(ntt_b200_context ctx, int op, size_t level, size_t batch,
+                             size_t *out);
+
+/* ModUp: Q_L (coefficient if src_is_eval == 0, else evaluation) -> evaluation
+ * QP. Replaces Session::mod_up (src/resident.cpp:431-447). */
+int ntt_b200_mod_up(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
+                    int src_is_eval, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ModDown: evaluation QP -> evaluation Q_L. Replaces Session::mod_down
+ * (src/resident.cpp:448-457). */
+int ntt_b200_mod_down(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+/* Hybrid digits: evaluation Q_L -> beta evaluation-QP digits (beta x (L+K)
+ * towers). Replaces Session::hybrid_digits (src/resident.cpp:458-491). */
+int ntt_b200_hybrid_digits(ntt_b200_context ctx, size_t level, uint64_t *digits,
+                           const uint64_t *src, void *workspace, size_t workspace_bytes,
+                           void *stream);
+
+/* Full Hybrid key switch of one evaluation-Q_L component `src`: digits, MAC
+ * with the full-context key, optional rotation (c0 != NULL: P*c0 added and
+ * the automorphism applied to the extended QP result), ModDown of both
+ * channels. Outputs evaluation Q_L. Replaces run_hybrid_core
+ * (include/ntt/openfhe_hybrid_adapter.hpp:163-181). */
+int ntt_b200_keyswitch(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                       const uint64_t *src, const uint64_t *key_b, const uint64_t *key_a,
+                       const uint64_t *c0, uint32_t automorphism, void *workspace,
+                       size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,245 @@
+"""B200 (sm_100a) CKKS NTT / ModUp / ModDown / Hybrid key-switch path.
+
+Python access to the C ABI of include/ntt_b200.h (libntt_b200.so, built in
+tree by ntt_gpu_b200/build.py). Device buffers are torch CUDA tensors of dtype
+int64 holding u64 residues bit-for-bit; streams are torch CUDA streams. The
+CUDA library is the only implementation: there is no CPU fallback, and loading
+fails loudly when the library is missing.
+
+Errors follow the reference's conventions (include/ntt/backend_contract.hpp:20-26,
+src/cuda/ntt_kernels.cu:40-46): invalid arguments raise ContractError (a
+ValueError) before anything is enqueued; CUDA failures raise CudaError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .build import LIB
+
+__all__ = ["ContractError", "CudaError", "WorkspaceError", "Context", "library", "load",
+           "kernel_launches", "OP_MOD_UP", "OP_MOD_DOWN", "OP_DIGITS", "OP_KEYSWITCH"]
+
+OK, ERR_CONTRACT, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_TIMEOUT = range(6)
+OP_MOD_UP, OP_MOD_DOWN, OP_DIGITS, OP_KEYSWITCH = 1, 2, 3, 4
+
+
+class ContractError(ValueError):
+    """Invalid argument or layout; raised before any device work is enqueued."""
+
+
+class CudaError(RuntimeError):
+    """CUDA runtime failure."""
+
+
+class WorkspaceError(ValueError):
+    """Workspace missing or too small."""
+
+
+class TimeoutError_(RuntimeError):
+    """A bounded device wait expired."""
+
+
+_lib = None
+_U64, _SZ, _P, _I = ctypes.c_uint64, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int
+
+_SIGNATURES = {
+    "ntt_b200_last_error": ([], ctypes.c_char_p),
+    "ntt_b200_kernel_launches": ([], _U64),
+    "ntt_b200_context_create": ([ctypes.POINTER(_P), _I, _U64, _P, _P, _SZ, _P, _P, _SZ, _SZ], _I),
+    "ntt_b200_context_destroy": ([_P], _I),
+    "ntt_b200_context_table_bytes": ([_P, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_context_prepare": ([_P, _SZ], _I),
+    "ntt_b200_ntt": ([_P, _P, _P, _P, _SZ, _SZ, _SZ, _I, _P], _I),
+    "ntt_b200_pointwise": ([_P, _P, _P, _P, _P, _SZ, _SZ, _SZ, _P], _I),
+    "ntt_b200_switch_basis": ([_P, _P, _P, _P, _SZ, _P, _SZ, _P], _I),
+    "ntt_b200_correct": ([_P, _SZ, _P, _P, _P, _P], _I),
+    "ntt_b200_hybrid_mac": ([_P, _SZ, _P, _P, _P, _P, _P, _P], _I),
+    "ntt_b200_hybrid_rotate": ([_P, _SZ, _P, _P, _P, _P, _P, ctypes.c_uint32, _P], _I),
+    "ntt_b200_workspace_bytes": ([_P, _I, _SZ, _SZ, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_mod_up": ([_P, _SZ, _P, _P, _I, _P, _SZ, _P], _I),
+    "ntt_b200_mod_down": ([_P, _SZ, _P, _P, _P, _SZ, _P], _I),
+    "ntt_b200_hybrid_digits": ([_P, _SZ, _P, _P, _P, _SZ, _P], _I),
+    "ntt_b200_keyswitch": ([_P, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
+}
+
+
+def load(path: str = LIB):
+    """Load libntt_b200.so and bind every entry point of include/ntt_b200.h."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libntt_b200.so not built at {path}; run ntt_gpu_b200/build.py")
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def library():
+    return load()
+
+
+def kernel_launches() -> int:
+    return int(load().ntt_b200_kernel_launches())
+
+
+def _check(rc: int):
+    if rc == OK:
+        return
+    msg = load().ntt_b200_last_error().decode()
+    if rc == ERR_CONTRACT or rc == ERR_UNSUPPORTED:
+        raise ContractError(msg)
+    if rc == ERR_WORKSPACE:
+        raise WorkspaceError(msg)
+    if rc == ERR_TIMEOUT:
+        raise TimeoutError_(msg)
+    raise CudaError(msg)
+
+
+def _arr(values, ctype=_U64):
+    values = [int(v) for v in values]
+    return (ctype * max(1, len(values)))(*values)
+
+
+def _ptr(t) -> int | None:
+    """Device address of a torch tensor (or None)."""
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "expected a contiguous CUDA tensor"
+    return t.data_ptr()
+
+
+def _stream(stream) -> int | None:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+class Context:
+    """One CKKS context (N, M Q towers, K P towers, alpha) with HBM tables.
+
+    Tower ids: Q tower i -> i, P tower j -> M + j.
+    """
+
+    def __init__(self, n, q, q_psi, p=(), p_psi=(), alpha=1, device=0):
+        lib = load()
+        self.n, self.m, self.k, self.alpha, self.device = int(n), len(q), len(p), int(alpha), int(device)
+        self.q, self.q_psi, self.p, self.p_psi = list(q), list(q_psi), list(p), list(p_psi)
+        handle = _P()
+        _check(lib.ntt_b200_context_create(ctypes.byref(handle), self.device, self.n, _arr(q), _arr(q_psi),
+                                           self.m, _arr(p), _arr(p_psi), self.k, self.alpha))
+        self._h = handle
+        self._lib = lib
+
+    @classmethod
+    def from_oracle(cls, ctx, device=0):
+        return cls(ctx.n, ctx.q, ctx.q_psi, ctx.p, ctx.p_psi, ctx.alpha, device)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(self._lib.ntt_b200_context_destroy(self._h))
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- helpers -----------------------------------------------------------------
+    def digits(self, level):
+        return 1 + (level - 1) // self.alpha
+
+    def full_digits(self):
+        return 1 + (self.m - 1) // self.alpha
+
+    def qp_ids(self, level):
+        return list(range(level)) + [self.m + j for j in range(self.k)]
+
+    def table_bytes(self) -> int:
+        out = _SZ()
+        _check(self._lib.ntt_b200_context_table_bytes(self._h, ctypes.byref(out)))
+        return out.value
+
+    def prepare(self, level):
+        _check(self._lib.ntt_b200_context_prepare(self._h, level))
+
+    def workspace_bytes(self, op, level, batch=1) -> int:
+        out = _SZ()
+        _check(self._lib.ntt_b200_workspace_bytes(self._h, op, level, batch, ctypes.byref(out)))
+        return out.value
+
+    def workspace(self, op, level, batch=1):
+        import torch
+        nbytes = self.workspace_bytes(op, level, batch)
+        return torch.empty(max(1, (nbytes + 7) // 8), dtype=torch.int64, device=f"cuda:{self.device}")
+
+    # ---- primitives ---------------------------------------------------------------
+    def ntt(self, dst, src, tower_ids, polys=1, poly_stride=0, inverse=False, stream=None):
+        _check(self._lib.ntt_b200_ntt(self._h, _ptr(dst), _ptr(src), _arr(tower_ids, ctypes.c_uint32),
+                                      len(tower_ids), polys, poly_stride, int(inverse), _stream(stream)))
+
+    def pointwise(self, dst, left, right, tower_ids, polys=1, poly_stride=0, stream=None):
+        _check(self._lib.ntt_b200_pointwise(self._h, _ptr(dst), _ptr(left), _ptr(right),
+                                            _arr(tower_ids, ctypes.c_uint32), len(tower_ids), polys,
+                                            poly_stride, _stream(stream)))
+
+    def switch_basis(self, dst, src, source_ids, target_ids, stream=None):
+        _check(self._lib.ntt_b200_switch_basis(self._h, _ptr(dst), _ptr(src),
+                                               _arr(source_ids, ctypes.c_uint32), len(source_ids),
+                                               _arr(target_ids, ctypes.c_uint32), len(target_ids),
+                                               _stream(stream)))
+
+    def correct(self, level, dst, left, right, stream=None):
+        _check(self._lib.ntt_b200_correct(self._h, level, _ptr(dst), _ptr(left), _ptr(right), _stream(stream)))
+
+    def hybrid_mac(self, level, out_b, out_a, digits, key_b, key_a, stream=None):
+        _check(self._lib.ntt_b200_hybrid_mac(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(digits),
+                                             _ptr(key_b), _ptr(key_a), _stream(stream)))
+
+    def hybrid_rotate(self, level, out_b, out_a, ext_b, ext_a, c0, automorphism, stream=None):
+        _check(self._lib.ntt_b200_hybrid_rotate(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(ext_b),
+                                                _ptr(ext_a), _ptr(c0), automorphism, _stream(stream)))
+
+    # ---- composites -----------------------------------------------------------------
+    def mod_up(self, level, dst, src, src_is_eval, workspace, stream=None):
+        _check(self._lib.ntt_b200_mod_up(self._h, level, _ptr(dst), _ptr(src), int(src_is_eval),
+                                         _ptr(workspace), workspace.numel() * 8, _stream(stream)))
+
+    def mod_down(self, level, dst, src, workspace, stream=None):
+        _check(self._lib.ntt_b200_mod_down(self._h, level, _ptr(dst), _ptr(src), _ptr(workspace),
+                                           workspace.numel() * 8, _stream(stream)))
+
+    def hybrid_digits(self, level, digits, src, workspace, stream=None):
+        _check(self._lib.ntt_b200_hybrid_digits(self._h, level, _ptr(digits), _ptr(src), _ptr(workspace),
+                                                workspace.numel() * 8, _stream(stream)))
+
+    def keyswitch(self, level, out_b, out_a, src, key_b, key_a, workspace, c0=None, automorphism=0,
+                  stream=None):
+        _check(self._lib.ntt_b200_keyswitch(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(src), _ptr(key_b),
+                                            _ptr(key_a), _ptr(c0), automorphism, _ptr(workspace),
+                                            workspace.numel() * 8, _stream(stream)))
+
+
+def to_device(array, device=0):
+    """numpy uint64 array -> CUDA int64 tensor with the same bits."""
+    import numpy as np
+    import torch
+    a = np.ascontiguousarray(array, dtype=np.uint64)
+    return torch.from_numpy(a.view(np.int64)).to(f"cuda:{device}")
+
+
+def to_host(tensor):
+    """CUDA int64 tensor -> numpy uint64 array with the same bits."""
+    import numpy as np
+    return tensor.detach().cpu().numpy().view(np.uint64)
+
+
+def empty(shape, device=0):
+    import torch
+    return torch.empty(shape, dtype=torch.int64, device=f"cuda:{device}")

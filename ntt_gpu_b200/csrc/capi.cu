@@ -1,0 +1,845 @@
+// C ABI of the B200 CKKS key-switch path (declarations in include/ntt_b200.h).
+// Host side: parameter validation, HBM-resident tables, plan caches and kernel
+// launches. Composite operations (ModUp, ModDown, Hybrid digits, key switch)
+// run on the caller's stream with a caller-provided workspace.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <initializer_list>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ntt_b200.h"
+#include "arith.cuh"
+#include "kernels.cuh"
+#include "ntt.cuh"
+#include "tables.cuh"
+
+using b200::u64;
+using u128 = unsigned __int128;
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+
+struct ContractError : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct WorkspaceError : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+void require(bool ok, const char *why) {
+  if (!ok) throw ContractError(why);
+}
+void check_cuda(cudaError_t e, const char *call) {
+  if (e != cudaSuccess) throw CudaError(std::string("CUDA: ") + call + ": " + cudaGetErrorString(e));
+}
+#define CUDA_CHECK(x) check_cuda((x), #x)
+
+template <class F> int guarded(F f) {
+  try {
+    f();
+    return NTT_B200_OK;
+  } catch (const WorkspaceError &e) {
+    g_last_error = e.what();
+    return NTT_B200_ERR_WORKSPACE;
+  } catch (const ContractError &e) {
+    g_last_error = e.what();
+    return NTT_B200_ERR_CONTRACT;
+  } catch (const CudaError &e) {
+    g_last_error = e.what();
+    return NTT_B200_ERR_CUDA;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return NTT_B200_ERR_CUDA;
+  }
+}
+
+// ---- host integer arithmetic -------------------------------------------------
+u64 h_mul(u64 a, u64 b, u64 q) { return (u64)(((u128)a * b) % q); }
+u64 h_pow(u64 a, u64 e, u64 q) {
+  u64 r = 1 % q, b = a % q;
+  for (; e; e >>= 1) {
+    if (e & 1) r = h_mul(r, b, q);
+    b = h_mul(b, b, q);
+  }
+  return r;
+}
+u64 h_inv(u64 x, u64 q) {
+  require(x % q != 0, "inverse of zero");
+  return h_pow(x, q - 2, q);
+}
+u64 h_shoup(u64 w, u64 q) { return (u64)(((u128)w << 64) / q); }
+b200::Shoup h_shoup_pair(u64 w, u64 q) { return {w, h_shoup(w, q)}; }
+bool h_is_prime(u64 n) {
+  static const u64 bases[12] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+  if (n < 2) return false;
+  for (u64 p : bases)
+    if (n % p == 0) return n == p;
+  u64 d = n - 1, s = 0;
+  while (!(d & 1)) d >>= 1, ++s;
+  for (u64 a : bases) {
+    u64 x = h_pow(a, d, n);
+    if (x == 1 || x == n - 1) continue;
+    bool composite = true;
+    for (u64 r = 1; r < s; ++r) {
+      x = h_mul(x, x, n);
+      if (x == n - 1) {
+        composite = false;
+        break;
+      }
+    }
+    if (composite) return false;
+  }
+  return true;
+}
+uint32_t h_bitrev(uint32_t x, int bits) {
+  uint32_t r = 0;
+  for (int i = 0; i < bits; ++i) r = (r << 1) | ((x >> i) & 1);
+  return r;
+}
+b200::Reducer h_reducer(u64 m) {
+  b200::Reducer r;
+  r.m = m;
+  r.one = h_shoup(1, m);
+  r.r64 = (u64)(((u128)1 << 64) % m);
+  r.r64q = h_shoup(r.r64, m);
+  r.r128 = h_mul(r.r64, r.r64, m);
+  r.r128q = h_shoup(r.r128, m);
+  return r;
+}
+
+struct DeviceGuard {
+  int previous = -1;
+  explicit DeviceGuard(int device) {
+    CUDA_CHECK(cudaGetDevice(&previous));
+    if (previous != device) CUDA_CHECK(cudaSetDevice(device));
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    if (cudaGetDevice(&now) == cudaSuccess && now != previous) cudaSetDevice(previous);
+  }
+};
+
+struct HostConvPlan {
+  b200::ConvPlan *device = nullptr;
+  int s = 0, t = 0;
+  bool wide = false;
+};
+}  // namespace
+
+struct ntt_b200_context_s {
+  int device = 0;
+  u64 n = 0;
+  int logn = 0;
+  size_t m = 0, k = 0, alpha = 0;
+  bool lazy = true;
+  std::vector<u64> mod, psi;  // [M + K] by global id
+  b200::TowerConsts *d_tc = nullptr;
+  ulonglong2 *d_fwd = nullptr, *d_inv = nullptr;
+  b200::DeviceTables tables{};
+  size_t table_bytes = 0;
+  std::mutex mu;
+  std::map<std::pair<std::vector<uint16_t>, std::vector<uint16_t>>, HostConvPlan> conv;
+  std::map<size_t, b200::DownPlan *> down;
+
+  size_t towers() const { return m + k; }
+
+  ~ntt_b200_context_s() {
+    // Destruction requires quiescence: the caller has synchronised every stream
+    // that used this context (the reference frees tables only after proven
+    // quiescence, src/cuda/resident_adapter.inc:107-115).
+    for (auto &kv : conv) cudaFree(kv.second.device);
+    for (auto &kv : down) cudaFree(kv.second);
+    cudaFree(d_tc);
+    cudaFree(d_fwd);
+    cudaFree(d_inv);
+  }
+
+  const HostConvPlan &conv_plan(const std::vector<uint16_t> &src, const std::vector<uint16_t> &tgt) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(src, tgt);
+    auto it = conv.find(key);
+    if (it != conv.end()) return it->second;
+    require(!src.empty() && src.size() <= (size_t)b200::kMaxConvSources, "basis switch requires 1..40 source towers");
+    require(!tgt.empty() && tgt.size() <= (size_t)b200::kMaxConvTargets, "basis switch requires 1..80 target towers");
+    std::vector<uint16_t> all(src);
+    all.insert(all.end(), tgt.begin(), tgt.end());
+    for (auto id : all) require(id < towers(), "tower id out of range");
+    std::sort(all.begin(), all.end());
+    require(std::adjacent_find(all.begin(), all.end()) == all.end(), "basis switch requires distinct disjoint towers");
+    auto plan = std::make_unique<b200::ConvPlan>();
+    std::memset(plan.get(), 0, sizeof(b200::ConvPlan));
+    const int s = (int)src.size(), t = (int)tgt.size();
+    plan->s = s;
+    plan->t = t;
+    u64 max_src = 0, max_tgt = 0;
+    for (int j = 0; j < s; ++j) {
+      const u64 b = mod[src[j]];
+      u64 hat = 1;
+      for (int o = 0; o < s; ++o)
+        if (o != j) hat = h_mul(hat, mod[src[o]] % b, b);
+      plan->src_q[j] = b;
+      plan->src_inv[j] = h_shoup_pair(h_inv(hat, b), b);
+      plan->src_id[j] = src[j];
+      max_src = std::max(max_src, b);
+      for (int i = 0; i < t; ++i) {
+        const u64 m_i = mod[tgt[i]];
+        u64 h = 1;
+        for (int o = 0; o < s; ++o)
+          if (o != j) h = h_mul(h, mod[src[o]] % m_i, m_i);
+        plan->hat[j * t + i] = h;
+      }
+    }
+    for (int i = 0; i < t; ++i) {
+      plan->tgt_id[i] = tgt[i];
+      plan->tgt[i] = h_reducer(mod[tgt[i]]);
+      max_tgt = std::max(max_tgt, mod[tgt[i]]);
+    }
+    HostConvPlan hp;
+    hp.s = s;
+    hp.t = t;
+    const u128 prod = (u128)(max_src - 1) * (max_tgt - 1);
+    hp.wide = prod > (~(u128)0) / (u128)s;
+    DeviceGuard guard(device);
+    CUDA_CHECK(cudaMalloc(&hp.device, sizeof(b200::ConvPlan)));
+    CUDA_CHECK(cudaMemcpy(hp.device, plan.get(), sizeof(b200::ConvPlan), cudaMemcpyHostToDevice));
+    return conv.emplace(key, hp).first->second;
+  }
+
+  b200::DownPlan *down_plan(size_t level) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = down.find(level);
+    if (it != down.end()) return it->second;
+    b200::DownPlan host{};
+    for (size_t t = 0; t < level; ++t) {
+      const u64 q = mod[t];
+      u64 prod = 1;
+      for (size_t j = 0; j < k; ++j) prod = h_mul(prod, mod[m + j] % q, q);
+      host.p_inv[t] = h_shoup_pair(h_inv(prod, q), q);
+      host.p_mod[t] = h_shoup_pair(prod, q);
+    }
+    b200::DownPlan *d = nullptr;
+    DeviceGuard guard(device);
+    CUDA_CHECK(cudaMalloc(&d, sizeof(b200::DownPlan)));
+    CUDA_CHECK(cudaMemcpy(d, &host, sizeof(b200::DownPlan), cudaMemcpyHostToDevice));
+    return down.emplace(level, d).first->second;
+  }
+};
+
+namespace {
+using Ctx = ntt_b200_context_s;
+
+void require_ctx(const Ctx *c) { require(c != nullptr, "null context"); }
+void require_level(const Ctx *c, size_t level, bool need_p = true) {
+  require(level >= 1 && level <= c->m, "invalid active Q count");
+  require(!need_p || c->k > 0, "QP requires P towers");
+  require(level <= 40 && c->k <= 40, "conversion requires 1..40 active Q and P towers");
+}
+cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+// Kernels move tower data with 16-byte vector accesses.
+void require_aligned(std::initializer_list<const void *> ptrs) {
+  for (const void *p : ptrs)
+    require(p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15) == 0,
+            "device pointers must be 16-byte aligned");
+}
+
+void after_launch(int count = 1) {
+  CUDA_CHECK(cudaGetLastError());
+  g_launches += count;
+}
+
+// ---- NTT launches ----------------------------------------------------------------
+struct Slot {
+  uint32_t off;
+  uint16_t id;
+};
+
+template <int LOGN, bool LAZY>
+void launch_ntt_2pass(const Ctx &c, u64 *dst, const u64 *src, const b200::NttBatch &b, int slots,
+                      int polys, bool inverse, cudaStream_t st) {
+  const dim3 grid((1u << LOGN) / b200::kTileWords, slots, polys);
+  b200::NttBatch first = b;
+  first.src = src;
+  first.dst = dst;
+  b200::NttBatch second = b;
+  second.src = dst;
+  second.dst = dst;
+  if (!inverse) {
+    b200::ntt_fwd_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(first, c.tables);
+    b200::ntt_fwd_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+  } else {
+    b200::ntt_inv_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(first, c.tables);
+    b200::ntt_inv_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+  }
+  after_launch(2);
+}
+
+template <bool LAZY>
+void launch_ntt_chunk(const Ctx &c, u64 *dst, const u64 *src, const b200::NttBatch &b, int slots,
+                      int polys, bool inverse, cudaStream_t st) {
+  switch (c.logn) {
+    case 12: launch_ntt_2pass<12, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
+    case 13: launch_ntt_2pass<13, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
+    case 14: launch_ntt_2pass<14, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
+    case 15: launch_ntt_2pass<15, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
+    case 16: launch_ntt_2pass<16, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
+    default: throw ContractError("unsupported ring dimension");
+  }
+}
+
+// NTT of a list of slots; each slot is (tower offset from base, global id).
+void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots, size_t polys,
+             u64 poly_stride, bool inverse, cudaStream_t st) {
+  require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
+  for (size_t first = 0; first < slots.size(); first += b200::kMaxSlots) {
+    const size_t count = std::min<size_t>(b200::kMaxSlots, slots.size() - first);
+    b200::NttBatch b{};
+    b.poly_stride = poly_stride;
+    for (size_t i = 0; i < count; ++i) {
+      b.off[i] = slots[first + i].off;
+      b.id[i] = slots[first + i].id;
+    }
+    b.src = src;
+    b.dst = dst;
+    if (c.logn <= 11) {
+      const dim3 grid(1, (unsigned)count, (unsigned)polys);
+      const int threads = std::min<int>(b200::kNttThreads, std::max<int>(32, (int)(c.n / 2)));
+      if (inverse)
+        b200::ntt_small<true><<<grid, threads, 0, st>>>(b, c.tables);
+      else
+        b200::ntt_small<false><<<grid, threads, 0, st>>>(b, c.tables);
+      after_launch();
+    } else if (c.lazy) {
+      launch_ntt_chunk<true>(c, dst, src, b, (int)count, (int)polys, inverse, st);
+    } else {
+      launch_ntt_chunk<false>(c, dst, src, b, (int)count, (int)polys, inverse, st);
+    }
+  }
+}
+
+std::vector<Slot> contiguous_slots(const std::vector<uint16_t> &ids, uint32_t first_off = 0) {
+  std::vector<Slot> s;
+  for (size_t i = 0; i < ids.size(); ++i) s.push_back({first_off + (uint32_t)i, ids[i]});
+  return s;
+}
+std::vector<uint16_t> range_ids(size_t begin, size_t end) {
+  std::vector<uint16_t> v;
+  for (size_t i = begin; i < end; ++i) v.push_back((uint16_t)i);
+  return v;
+}
+std::vector<uint16_t> qp_ids(const Ctx &c, size_t level) {
+  auto v = range_ids(0, level);
+  for (size_t j = 0; j < c.k; ++j) v.push_back((uint16_t)(c.m + j));
+  return v;
+}
+
+// ---- conversion launches ---------------------------------------------------------
+template <int MAXS>
+void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, cudaStream_t st) {
+  if (p.wide)
+    b200::conv_kernel<MAXS, true><<<grid, b200::kEwThreads, 0, st>>>(a);
+  else
+    b200::conv_kernel<MAXS, false><<<grid, b200::kEwThreads, 0, st>>>(a);
+}
+void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
+              const std::vector<uint16_t> &slots, size_t polys, u64 src_stride, u64 dst_stride,
+              cudaStream_t st) {
+  b200::ConvArgs a{};
+  a.plan = p.device;
+  a.src = src;
+  a.dst = dst;
+  a.src_poly_stride = src_stride;
+  a.dst_poly_stride = dst_stride;
+  for (size_t i = 0; i < slots.size(); ++i) a.slot[i] = slots[i];
+  a.logn = c.logn;
+  a.targets_per_block = 8;
+  const dim3 grid((unsigned)((c.n + b200::kEwThreads - 1) / b200::kEwThreads),
+                  (unsigned)((p.t + a.targets_per_block - 1) / a.targets_per_block), (unsigned)polys);
+  if (p.s <= 4) launch_conv_t<4>(p, a, grid, st);
+  else if (p.s <= 8) launch_conv_t<8>(p, a, grid, st);
+  else if (p.s <= 16) launch_conv_t<16>(p, a, grid, st);
+  else launch_conv_t<40>(p, a, grid, st);
+  after_launch();
+}
+
+dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
+  return dim3((unsigned)((c.n + b200::kEwThreads - 1) / b200::kEwThreads), (unsigned)towers,
+              (unsigned)polys);
+}
+
+// ---- workspace carving -----------------------------------------------------------
+struct Carver {
+  char *base;
+  size_t size, used = 0;
+  u64 *take(size_t words) {
+    const size_t bytes = ((words * sizeof(u64)) + 255) / 256 * 256;
+    if (used + bytes > size) throw WorkspaceError("workspace too small");
+    u64 *p = reinterpret_cast<u64 *>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+size_t aligned_words(size_t words) { return ((words * sizeof(u64)) + 255) / 256 * 256; }
+
+size_t workspace_bytes(const Ctx &c, int op, size_t level, size_t batch) {
+  const size_t n = c.n, L = level, K = c.k, T = L + K;
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  size_t bytes = 0;
+  switch (op) {
+    case NTT_B200_OP_MOD_UP: bytes = aligned_words(L * n); break;
+    case NTT_B200_OP_MOD_DOWN: bytes = aligned_words(K * n) + aligned_words(L * n); break;
+    case NTT_B200_OP_DIGITS: bytes = aligned_words(L * n); break;
+    case NTT_B200_OP_KEYSWITCH:
+      bytes = aligned_words(beta * T * n) + aligned_words(L * n) + 2 * aligned_words(T * n) +
+              2 * aligned_words(T * n) + aligned_words(K * n) + aligned_words(L * n);
+      break;
+    default: throw ContractError("unknown workspace operation");
+  }
+  return bytes * batch;
+}
+
+// ---- composite operations (one request) -------------------------------------------
+void do_mod_down(Ctx &c, size_t L, u64 *dst, const u64 *src, Carver &ws, cudaStream_t st) {
+  const size_t n = c.n, K = c.k;
+  u64 *p_coeff = ws.take(K * n);
+  u64 *corr = ws.take(L * n);
+  run_ntt(c, p_coeff, src + L * n, contiguous_slots(range_ids(c.m, c.m + K)), 1, 0, true, st);
+  const auto &plan = c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L));
+  std::vector<uint16_t> slots;
+  for (size_t i = 0; i < L; ++i) slots.push_back((uint16_t)i);
+  run_conv(c, plan, corr, p_coeff, slots, 1, 0, 0, st);
+  run_ntt(c, corr, corr, contiguous_slots(range_ids(0, L)), 1, 0, false, st);
+  b200::CorrectArgs a{};
+  a.dst = dst;
+  a.left = src;
+  a.right = corr;
+  a.plan = c.down_plan(L);
+  a.tc = c.d_tc;
+  a.towers = (int)L;
+  a.logn = c.logn;
+  b200::correct_kernel<<<ew_grid(c, L, 1), b200::kEwThreads, 0, st>>>(a);
+  after_launch();
+}
+
+void do_digits(Ctx &c, size_t L, u64 *digits, const u64 *src, Carver &ws, cudaStream_t st) {
+  const size_t n = c.n, K = c.k, T = L + K;
+  u64 *coeff = ws.take(L * n);
+  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), 1, 0, true, st);
+  const auto all = qp_ids(c, L);
+  std::vector<Slot> fwd;
+  size_t digit = 0;
+  for (size_t first = 0; first < L; first += c.alpha, ++digit) {
+    const size_t count = std::min(c.alpha, L - first);
+    u64 *out = digits + digit * T * n;
+    CUDA_CHECK(cudaMemcpyAsync(out + first * n, src + first * n, count * n * sizeof(u64),
+                               cudaMemcpyDeviceToDevice, st));
+    std::vector<uint16_t> tgt, slots;
+    for (size_t t = 0; t < T; ++t)
+      if (t < first || t >= first + count) {
+        tgt.push_back(all[t]);
+        slots.push_back((uint16_t)t);
+        fwd.push_back({(uint32_t)(digit * T + t), all[t]});
+      }
+    const auto &plan = c.conv_plan(range_ids(first, first + count), tgt);
+    run_conv(c, plan, out, coeff + first * n, slots, 1, 0, 0, st);
+  }
+  run_ntt(c, digits, digits, fwd, 1, 0, false, st);
+}
+
+void do_mac(Ctx &c, size_t L, u64 *out_b, u64 *out_a, const u64 *digits, const u64 *key_b,
+            const u64 *key_a, cudaStream_t st) {
+  const size_t n = c.n, T = L + c.k;
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  b200::MacArgs a{};
+  a.out_b = out_b;
+  a.out_a = out_a;
+  a.digits = digits;
+  a.key_b = key_b;
+  a.key_a = key_a;
+  a.tc = c.d_tc;
+  a.digit_stride = T * n;
+  a.key_digit_stride = c.towers() * n;
+  a.level = (int)L;
+  a.m = (int)c.m;
+  a.beta = (int)beta;
+  a.logn = c.logn;
+  u64 max_q = 0;
+  for (auto q : c.mod) max_q = std::max(max_q, q);
+  const u128 prod = (u128)(max_q - 1) * (max_q - 1);
+  const bool wide = prod > (~(u128)0) / (u128)beta;
+  if (wide)
+    b200::mac_kernel<true><<<ew_grid(c, T, 1), b200::kEwThreads, 0, st>>>(a);
+  else
+    b200::mac_kernel<false><<<ew_grid(c, T, 1), b200::kEwThreads, 0, st>>>(a);
+  after_launch();
+}
+
+void do_rotate(Ctx &c, size_t L, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,
+               const u64 *c0, uint32_t g, cudaStream_t st) {
+  require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
+  b200::RotateArgs a{};
+  a.out_b = out_b;
+  a.out_a = out_a;
+  a.ext_b = ext_b;
+  a.ext_a = ext_a;
+  a.c0 = c0;
+  a.plan = c.down_plan(L);
+  a.tc = c.d_tc;
+  a.level = (int)L;
+  a.m = (int)c.m;
+  a.logn = c.logn;
+  a.g = g;
+  b200::rotate_kernel<<<ew_grid(c, L + c.k, 1), b200::kEwThreads, 0, st>>>(a);
+  after_launch();
+}
+
+Carver carve(const Ctx &c, void *ws, size_t bytes, int op, size_t level) {
+  const size_t need = workspace_bytes(c, op, level, 1);
+  if (need && (!ws || bytes < need)) throw WorkspaceError("workspace missing or too small");
+  return Carver{reinterpret_cast<char *>(ws), bytes};
+}
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+const char *ntt_b200_last_error(void) { return g_last_error.c_str(); }
+uint64_t ntt_b200_kernel_launches(void) { return g_launches.load(); }
+
+int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const uint64_t *q,
+                            const uint64_t *q_psi, size_t m, const uint64_t *p,
+                            const uint64_t *p_psi, size_t k, size_t alpha) {
+  return guarded([&] {
+    require(out != nullptr, "null output handle");
+    *out = nullptr;
+    require(n >= 2 && (n & (n - 1)) == 0 && n <= 65536, "ring dimension must be a power of two in [2, 65536]");
+    require(m >= 1 && q && q_psi, "missing Q towers");
+    require(alpha >= 1 && alpha <= m, "invalid Q/digit geometry");
+    require(k == 0 || (p && p_psi), "missing P towers");
+    require(m + k <= (size_t)b200::kMaxTowers, "at most 128 towers per context");
+    require(device >= 0, "invalid device ordinal");
+    auto c = std::make_unique<Ctx>();
+    c->device = device;
+    c->n = n;
+    while ((u64(1) << c->logn) < n) ++c->logn;
+    c->m = m;
+    c->k = k;
+    c->alpha = alpha;
+    for (size_t i = 0; i < m + k; ++i) {
+      const u64 mq = i < m ? q[i] : p[i - m];
+      const u64 ps = i < m ? q_psi[i] : p_psi[i - m];
+      require(mq > n && mq < (u64(1) << 63) && mq % (2 * n) == 1, "invalid modulus shape");
+      require(h_is_prime(mq), "composite modulus");
+      require(ps > 0 && ps < mq && h_pow(ps, n, mq) == mq - 1, "invalid primitive root");
+      require(std::find(c->mod.begin(), c->mod.end(), mq) == c->mod.end(), "duplicate Q/P modulus");
+      c->mod.push_back(mq);
+      c->psi.push_back(ps);
+      if (mq >= (u64(1) << 62)) c->lazy = false;
+    }
+    const size_t T = m + k;
+    std::vector<b200::TowerConsts> tc(T);
+    std::vector<ulonglong2> fwd(T * n), inv(T * n);
+    std::vector<u64> pw(n);
+    for (size_t g = 0; g < T; ++g) {
+      const u64 mq = c->mod[g];
+      const u64 root = c->psi[g], root_inv = h_inv(root, mq);
+      for (int pass = 0; pass < 2; ++pass) {
+        const u64 r = pass ? root_inv : root;
+        u64 acc = 1;
+        for (u64 e = 0; e < n; ++e) {
+          pw[e] = acc;
+          acc = h_mul(acc, r, mq);
+        }
+        ulonglong2 *dst = (pass ? inv.data() : fwd.data()) + g * n;
+        for (u64 e = 0; e < n; ++e) {
+          const u64 w = pw[e];
+          const uint32_t idx = h_bitrev((uint32_t)e, c->logn);
+          dst[idx] = make_ulonglong2(w, h_shoup(w, mq));
+        }
+      }
+      const u64 ninv = h_inv(n % mq, mq);
+      tc[g].q = mq;
+      tc[g].q2 = 2 * mq;
+      tc[g].ninv = h_shoup_pair(ninv, mq);
+      tc[g].last_inv = h_shoup_pair(h_mul(inv[g * n + 1].x, ninv, mq), mq);
+      tc[g].red = h_reducer(mq);
+    }
+    DeviceGuard guard(device);
+    CUDA_CHECK(cudaMalloc(&c->d_tc, T * sizeof(b200::TowerConsts)));
+    CUDA_CHECK(cudaMalloc(&c->d_fwd, T * n * sizeof(ulonglong2)));
+    CUDA_CHECK(cudaMalloc(&c->d_inv, T * n * sizeof(ulonglong2)));
+    CUDA_CHECK(cudaMemcpy(c->d_tc, tc.data(), T * sizeof(b200::TowerConsts), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(c->d_fwd, fwd.data(), T * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(c->d_inv, inv.data(), T * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    c->tables = b200::DeviceTables{c->d_tc, c->d_fwd, c->d_inv, c->logn};
+    c->table_bytes = T * sizeof(b200::TowerConsts) + 2 * T * n * sizeof(ulonglong2);
+    *out = c.release();
+  });
+}
+
+int ntt_b200_context_destroy(ntt_b200_context ctx) {
+  return guarded([&] {
+    if (!ctx) return;
+    DeviceGuard guard(ctx->device);
+    delete ctx;
+  });
+}
+
+int ntt_b200_context_table_bytes(ntt_b200_context ctx, size_t *out) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(out != nullptr, "null output");
+    *out = ctx->table_bytes;
+  });
+}
+
+int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    Ctx &c = *ctx;
+    const size_t L = level, K = c.k;
+    c.conv_plan(range_ids(0, L), range_ids(c.m, c.m + K));
+    c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L));
+    c.down_plan(L);
+    const auto all = qp_ids(c, L);
+    for (size_t first = 0; first < L; first += c.alpha) {
+      const size_t count = std::min(c.alpha, L - first);
+      std::vector<uint16_t> tgt;
+      for (size_t t = 0; t < L + K; ++t)
+        if (t < first || t >= first + count) tgt.push_back(all[t]);
+      c.conv_plan(range_ids(first, first + count), tgt);
+    }
+  });
+}
+
+int ntt_b200_ntt(ntt_b200_context ctx, uint64_t *dst, const uint64_t *src, const uint32_t *tower_ids,
+                 size_t towers, size_t polys, size_t poly_stride, int inverse, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(dst && src && tower_ids, "null pointer");
+    require_aligned({dst, src});
+    require(poly_stride % 2 == 0, "polynomial stride must be even");
+    require(towers >= 1 && polys >= 1, "empty transform batch");
+    require(polys == 1 || poly_stride >= towers * ctx->n, "overlapping polynomial stride");
+    std::vector<Slot> slots;
+    for (size_t i = 0; i < towers; ++i) {
+      require(tower_ids[i] < ctx->towers(), "tower id out of range");
+      slots.push_back({(uint32_t)i, (uint16_t)tower_ids[i]});
+    }
+    DeviceGuard guard(ctx->device);
+    run_ntt(*ctx, dst, src, slots, polys, poly_stride, inverse != 0, as_stream(stream));
+  });
+}
+
+int ntt_b200_pointwise(ntt_b200_context ctx, uint64_t *dst, const uint64_t *left,
+                       const uint64_t *right, const uint32_t *tower_ids, size_t towers,
+                       size_t polys, size_t poly_stride, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(dst && left && right && tower_ids, "null pointer");
+    require_aligned({dst, left, right});
+    require(poly_stride % 2 == 0, "polynomial stride must be even");
+    require(towers >= 1 && towers <= (size_t)b200::kMaxTowers && polys >= 1 && polys <= 65535,
+            "pointwise batch out of range");
+    require(polys == 1 || poly_stride >= towers * ctx->n, "overlapping polynomial stride");
+    b200::PointwiseArgs a{};
+    a.dst = dst;
+    a.left = left;
+    a.right = right;
+    a.tc = ctx->d_tc;
+    a.poly_stride = poly_stride;
+    for (size_t i = 0; i < towers; ++i) {
+      require(tower_ids[i] < ctx->towers(), "tower id out of range");
+      a.id[i] = (uint16_t)tower_ids[i];
+    }
+    a.towers = (int)towers;
+    a.logn = ctx->logn;
+    DeviceGuard guard(ctx->device);
+    b200::pointwise_kernel<<<ew_grid(*ctx, towers, polys), b200::kEwThreads, 0, as_stream(stream)>>>(a);
+    after_launch();
+  });
+}
+
+int ntt_b200_switch_basis(ntt_b200_context ctx, uint64_t *dst, const uint64_t *src,
+                          const uint32_t *source_ids, size_t s, const uint32_t *target_ids,
+                          size_t t, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(dst && src && source_ids && target_ids, "null pointer");
+    require_aligned({dst, src});
+    require(s >= 1 && s <= 40 && t >= 1 && t <= 40, "basis switch requires 1..40 source and target towers");
+    std::vector<uint16_t> sv, tv, slots;
+    for (size_t i = 0; i < s; ++i) {
+      require(source_ids[i] < ctx->towers(), "tower id out of range");
+      sv.push_back((uint16_t)source_ids[i]);
+    }
+    for (size_t i = 0; i < t; ++i) {
+      require(target_ids[i] < ctx->towers(), "tower id out of range");
+      tv.push_back((uint16_t)target_ids[i]);
+      slots.push_back((uint16_t)i);
+    }
+    DeviceGuard guard(ctx->device);
+    const auto &plan = ctx->conv_plan(sv, tv);
+    run_conv(*ctx, plan, dst, src, slots, 1, 0, 0, as_stream(stream));
+  });
+}
+
+int ntt_b200_correct(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *left,
+                     const uint64_t *right, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(dst && left && right, "null pointer");
+    require_aligned({dst, left, right});
+    DeviceGuard guard(ctx->device);
+    b200::CorrectArgs a{};
+    a.dst = dst;
+    a.left = left;
+    a.right = right;
+    a.plan = ctx->down_plan(level);
+    a.tc = ctx->d_tc;
+    a.towers = (int)level;
+    a.logn = ctx->logn;
+    b200::correct_kernel<<<ew_grid(*ctx, level, 1), b200::kEwThreads, 0, as_stream(stream)>>>(a);
+    after_launch();
+  });
+}
+
+int ntt_b200_hybrid_mac(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                        const uint64_t *digits, const uint64_t *key_b, const uint64_t *key_a,
+                        void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(out_b && out_a && digits && key_b && key_a, "null pointer");
+    require_aligned({out_b, out_a, digits, key_b, key_a});
+    DeviceGuard guard(ctx->device);
+    do_mac(*ctx, level, out_b, out_a, digits, key_b, key_a, as_stream(stream));
+  });
+}
+
+int ntt_b200_hybrid_rotate(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                           const uint64_t *ext_b, const uint64_t *ext_a, const uint64_t *c0,
+                           uint32_t automorphism, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(out_b && out_a && ext_b && ext_a && c0, "null pointer");
+    require_aligned({out_b, out_a, ext_b, ext_a, c0});
+    DeviceGuard guard(ctx->device);
+    do_rotate(*ctx, level, out_b, out_a, ext_b, ext_a, c0, automorphism, as_stream(stream));
+  });
+}
+
+int ntt_b200_workspace_bytes(ntt_b200_context ctx, int op, size_t level, size_t batch, size_t *out) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(out != nullptr && batch >= 1, "invalid workspace query");
+    *out = workspace_bytes(*ctx, op, level, batch);
+  });
+}
+
+int ntt_b200_mod_up(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
+                    int src_is_eval, void *workspace, size_t workspace_bytes, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(dst && src, "null pointer");
+    require_aligned({dst, src, workspace});
+    Ctx &c = *ctx;
+    Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_MOD_UP, level);
+    DeviceGuard guard(c.device);
+    const cudaStream_t st = as_stream(stream);
+    const size_t n = c.n, L = level, K = c.k;
+    const u64 *coeff = src;
+    if (src_is_eval) {
+      u64 *tmp = ws.take(L * n);
+      run_ntt(c, tmp, src, contiguous_slots(range_ids(0, L)), 1, 0, true, st);
+      CUDA_CHECK(cudaMemcpyAsync(dst, src, L * n * sizeof(u64), cudaMemcpyDeviceToDevice, st));
+      coeff = tmp;
+    } else {
+      run_ntt(c, dst, src, contiguous_slots(range_ids(0, L)), 1, 0, false, st);
+    }
+    const auto &plan = c.conv_plan(range_ids(0, L), range_ids(c.m, c.m + K));
+    std::vector<uint16_t> slots;
+    for (size_t i = 0; i < K; ++i) slots.push_back((uint16_t)(L + i));
+    run_conv(c, plan, dst, coeff, slots, 1, 0, 0, st);
+    run_ntt(c, dst, dst, contiguous_slots(range_ids(c.m, c.m + K), (uint32_t)L), 1, 0, false, st);
+  });
+}
+
+int ntt_b200_mod_down(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
+                      void *workspace, size_t workspace_bytes, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(dst && src, "null pointer");
+    require_aligned({dst, src, workspace});
+    Carver ws = carve(*ctx, workspace, workspace_bytes, NTT_B200_OP_MOD_DOWN, level);
+    DeviceGuard guard(ctx->device);
+    do_mod_down(*ctx, level, dst, src, ws, as_stream(stream));
+  });
+}
+
+int ntt_b200_hybrid_digits(ntt_b200_context ctx, size_t level, uint64_t *digits, const uint64_t *src,
+                           void *workspace, size_t workspace_bytes, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(digits && src, "null pointer");
+    require_aligned({digits, src, workspace});
+    Carver ws = carve(*ctx, workspace, workspace_bytes, NTT_B200_OP_DIGITS, level);
+    DeviceGuard guard(ctx->device);
+    do_digits(*ctx, level, digits, src, ws, as_stream(stream));
+  });
+}
+
+int ntt_b200_keyswitch(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                       const uint64_t *src, const uint64_t *key_b, const uint64_t *key_a,
+                       const uint64_t *c0, uint32_t automorphism, void *workspace,
+                       size_t workspace_bytes, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(out_b && out_a && src && key_b && key_a, "null pointer");
+    require_aligned({out_b, out_a, src, key_b, key_a, c0, workspace});
+    Ctx &c = *ctx;
+    if (c0) require((automorphism & 1) && automorphism < 2 * c.n, "invalid negacyclic automorphism index");
+    Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_KEYSWITCH, level);
+    DeviceGuard guard(c.device);
+    const cudaStream_t st = as_stream(stream);
+    const size_t n = c.n, L = level, T = L + c.k;
+    const size_t beta = 1 + (L - 1) / c.alpha;
+    u64 *digits = ws.take(beta * T * n);
+    u64 *acc_b = ws.take(T * n);
+    u64 *acc_a = ws.take(T * n);
+    do_digits(c, L, digits, src, ws, st);
+    do_mac(c, L, acc_b, acc_a, digits, key_b, key_a, st);
+    const u64 *ext_b = acc_b, *ext_a = acc_a;
+    if (c0) {
+      u64 *rot_b = ws.take(T * n);
+      u64 *rot_a = ws.take(T * n);
+      do_rotate(c, L, rot_b, rot_a, acc_b, acc_a, c0, automorphism, st);
+      ext_b = rot_b;
+      ext_a = rot_a;
+    }
+    Carver md = ws;
+    do_mod_down(c, L, out_b, ext_b, md, st);
+    do_mod_down(c, L, out_a, ext_a, ws, st);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,376 @@
+// Negacyclic NTT kernels for sm_100a.
+//
+// Transform (identical outputs to the reference NegacyclicNtt,
+// include/ntt/ntt.hpp:96-158): forward maps natural coefficients to evaluations
+// at psi^(2j+1) stored in bit-reversed order; inverse maps them back and scales
+// by N^-1. The schedule is the group-twiddle Cooley-Tukey / Gentleman-Sande
+// pair of the reference's CUDA path (include/ntt/transform_stage.hpp:40-80):
+// stage s (m = 2^s groups) pairs j with j + N/2^(s+1) and uses twiddle
+// T[2^s + (j >> (logN - s))].
+//
+// B200 schedule. N = R x 256 (R = 2^(logN-8), 16 <= R <= 256) is split in two
+// passes over 4096-word (32 KiB) tiles, one CTA of 256 threads each:
+//   column pass: stages 0 .. logR-1 over R rows x (4096/R) columns,
+//   row pass:    stages logR .. logN-1 over 16 contiguous rows of 256 words.
+// Each thread keeps 16 words in registers and runs up to 4 stages there
+// (radix-16), exchanging through shared memory between register phases.
+// Global traffic is staged through shared memory so every load and store is a
+// coalesced 16-byte vector access. Forward = column pass then row pass; inverse
+// = row pass then column pass with N^-1 folded into its last butterfly.
+// Small transforms (N <= 2048) run one CTA per tower entirely in shared memory.
+#pragma once
+#include <cstdint>
+
+#include "arith.cuh"
+#include "tables.cuh"
+
+namespace b200 {
+
+constexpr int kNttThreads = 256;
+constexpr int kTileWords = 4096;
+constexpr int kRowPad = 272;  // 256 words + one pad word per 16
+
+// A batch of tower transforms: slot y (blockIdx.y) of polynomial z
+// (blockIdx.z) lives at base + z * poly_stride + off[y] * N and uses the tables
+// of global tower id[y].
+constexpr int kMaxSlots = 128;
+struct NttBatch {
+  u64 *dst;
+  const u64 *src;
+  u64 poly_stride;
+  uint32_t off[kMaxSlots];
+  uint16_t id[kMaxSlots];
+};
+
+struct TowerView {
+  const TowerConsts *c;
+  const ulonglong2 *tw;
+  const u64 *src;
+  u64 *dst;
+};
+
+__device__ __forceinline__ TowerView tower_view(const NttBatch &b, const DeviceTables &T, bool inv) {
+  const uint32_t slot = blockIdx.y;
+  const uint32_t g = b.id[slot];
+  const u64 n = u64(1) << T.logn;
+  const u64 offset = blockIdx.z * b.poly_stride + u64(b.off[slot]) * n;
+  TowerView v;
+  v.c = T.tc + g;
+  v.tw = (inv ? T.inv : T.fwd) + g * n;
+  v.src = b.src + offset;
+  v.dst = b.dst + offset;
+  return v;
+}
+
+__device__ __forceinline__ Shoup tw_load(const ulonglong2 *p) {
+  const ulonglong2 v = __ldg(p);
+  return Shoup{v.x, v.y};
+}
+
+// Coalesced copy of a [rows x width] global block (row stride `stride` words)
+// into shared memory with the given padded row pitch. width is a multiple of 2.
+template <int ROWS, int WIDTH, int PITCH, bool PAD16>
+__device__ __forceinline__ void load_block(u64 *smem, const u64 *g, u64 stride) {
+  constexpr int CHUNKS = ROWS * WIDTH / 2;
+  for (int j = threadIdx.x; j < CHUNKS; j += kNttThreads) {
+    const int r = j / (WIDTH / 2), c = (j % (WIDTH / 2)) * 2;
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(g + r * stride + c);
+    const int s = r * PITCH + c + (PAD16 ? (c >> 4) : 0);
+    smem[s] = v.x;
+    smem[s + 1] = v.y;
+  }
+}
+template <int ROWS, int WIDTH, int PITCH, bool PAD16>
+__device__ __forceinline__ void store_block(u64 *g, const u64 *smem, u64 stride) {
+  constexpr int CHUNKS = ROWS * WIDTH / 2;
+  for (int j = threadIdx.x; j < CHUNKS; j += kNttThreads) {
+    const int r = j / (WIDTH / 2), c = (j % (WIDTH / 2)) * 2;
+    const int s = r * PITCH + c + (PAD16 ? (c >> 4) : 0);
+    ulonglong2 v;
+    v.x = smem[s];
+    v.y = smem[s + 1];
+    *reinterpret_cast<ulonglong2 *>(g + r * stride + c) = v;
+  }
+}
+
+// ---- column pass -------------------------------------------------------------
+// Tile: R rows x COLS columns starting at column blockIdx.x * COLS.
+// Thread (c, u): c = tid % COLS, u = tid / COLS in [0, R/16).
+// Mapping A: element e is row e * (R/16) + u     (varies the top 4 row bits).
+// Mapping B: element e is row (u * 2^(8-logR) + (e >> (logR-4))) * (R/16) + (e & (R/16-1))
+//            (varies the low logR-4 row bits).
+template <int LOGN>
+struct ColGeom {
+  static constexpr int LR = LOGN - 8, R = 1 << LR, COLS = kTileWords / R, TPC = R / 16;
+  static constexpr int LO_BITS = LR - 4;
+  __device__ static int row_a(int e, int u) { return e * TPC + u; }
+  __device__ static int row_b(int e, int u) {
+    return ((u << (8 - LR)) + (e >> LO_BITS)) * TPC + (e & (TPC - 1));
+  }
+};
+
+template <int LOGN, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads) ntt_fwd_col(NttBatch b, DeviceTables T) {
+  using G = ColGeom<LOGN>;
+  constexpr int N = 1 << LOGN;
+  __shared__ u64 tile[kTileWords];
+  __shared__ ulonglong2 tw[G::R];
+  const TowerView v = tower_view(b, T, false);
+  const u64 q = v.c->q, q2 = v.c->q2;
+  for (int i = threadIdx.x; i < G::R; i += kNttThreads) tw[i] = v.tw[i];
+  const int col0 = blockIdx.x * G::COLS;
+  load_block<G::R, G::COLS, G::COLS, false>(tile, v.src + col0, N >> G::LR);
+  __syncthreads();
+  const int c = threadIdx.x % G::COLS, u = threadIdx.x / G::COLS;
+  u64 x[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+  // Stages 0..3: row bit logR-1-s == register bit 3-s; group = e >> (4-s).
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const int d = 8 >> s;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
+      ct_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+    }
+  }
+  if constexpr (G::LR > 4) {
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = tile[G::row_b(e, u) * G::COLS + c];
+    // Stages 4..logR-1: row bit logR-1-s == register bit logR-1-s.
+#pragma unroll
+    for (int s = 4; s < G::LR; ++s) {
+      const int d = 1 << (G::LR - 1 - s);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+        ct_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) tile[G::row_b(e, u) * G::COLS + c] = x[e];
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
+  }
+  __syncthreads();
+  store_block<G::R, G::COLS, G::COLS, false>(v.dst + col0, tile, N >> G::LR);
+}
+
+template <int LOGN, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads) ntt_inv_col(NttBatch b, DeviceTables T) {
+  using G = ColGeom<LOGN>;
+  constexpr int N = 1 << LOGN;
+  __shared__ u64 tile[kTileWords];
+  __shared__ ulonglong2 tw[G::R];
+  const TowerView v = tower_view(b, T, true);
+  const u64 q = v.c->q, q2 = v.c->q2;
+  for (int i = threadIdx.x; i < G::R; i += kNttThreads) tw[i] = v.tw[i];
+  const int col0 = blockIdx.x * G::COLS;
+  load_block<G::R, G::COLS, G::COLS, false>(tile, v.src + col0, N >> G::LR);
+  __syncthreads();
+  const int c = threadIdx.x % G::COLS, u = threadIdx.x / G::COLS;
+  u64 x[16];
+  if constexpr (G::LR > 4) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = tile[G::row_b(e, u) * G::COLS + c];
+    // Stages logR-1 .. 4: row bit logR-1-s == register bit logR-1-s.
+#pragma unroll
+    for (int s = G::LR - 1; s >= 4; --s) {
+      const int d = 1 << (G::LR - 1 - s);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+        gs_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) tile[G::row_b(e, u) * G::COLS + c] = x[e];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+  // Stages 3..1, then stage 0 with N^-1 folded in.
+#pragma unroll
+  for (int s = 3; s >= 1; --s) {
+    const int d = 8 >> s;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
+      gs_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+    }
+  }
+  const Shoup ninv = v.c->ninv, last = v.c->last_inv;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) gs_last<LAZY>(x[e], x[e + 8], ninv, last, q, q2);
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
+  __syncthreads();
+  store_block<G::R, G::COLS, G::COLS, false>(v.dst + col0, tile, N >> G::LR);
+}
+
+// ---- row pass ----------------------------------------------------------------
+// Tile: 16 rows x 256 words starting at row blockIdx.x * 16; thread (r, u),
+// r = tid / 16, u = tid % 16. Mapping A: element e is column e*16 + u.
+// Mapping B: element e is column u*16 + e. Shared rows are padded to 272 words
+// (one pad word per 16) so both mappings are bank-conflict free.
+__device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
+
+template <int LOGN, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads) ntt_fwd_row(NttBatch b, DeviceTables T) {
+  constexpr int LR = LOGN - 8;
+  __shared__ u64 tile[16 * kRowPad];
+  const TowerView v = tower_view(b, T, false);
+  const u64 q = v.c->q, q2 = v.c->q2;
+  const int row0 = blockIdx.x * 16;
+  load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
+  __syncthreads();
+  const int r = threadIdx.x / 16, u = threadIdx.x % 16;
+  const int row = row0 + r;
+  u64 *my = tile + r * kRowPad;
+  u64 x[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+  // Stages LR + s', s' = 0..3: column bit 7-s' == register bit 3-s'.
+#pragma unroll
+  for (int sp = 0; sp < 4; ++sp) {
+    const int s = LR + sp, d = 8 >> sp;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
+      ct_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
+  // Stages LR + s', s' = 4..7: column bit 7-s' == register bit 7-s'.
+#pragma unroll
+  for (int sp = 4; sp < 8; ++sp) {
+    const int s = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+      ct_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    if constexpr (LAZY) x[e] = reduce4(x[e], q, q2);
+    my[pad_col(u * 16 + e)] = x[e];
+  }
+  __syncthreads();
+  store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+}
+
+template <int LOGN, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads) ntt_inv_row(NttBatch b, DeviceTables T) {
+  constexpr int LR = LOGN - 8;
+  __shared__ u64 tile[16 * kRowPad];
+  const TowerView v = tower_view(b, T, true);
+  const u64 q = v.c->q, q2 = v.c->q2;
+  const int row0 = blockIdx.x * 16;
+  load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
+  __syncthreads();
+  const int r = threadIdx.x / 16, u = threadIdx.x % 16;
+  const int row = row0 + r;
+  u64 *my = tile + r * kRowPad;
+  u64 x[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
+  // Stages LR + s', s' = 7..4: column bit 7-s' == register bit 7-s'.
+#pragma unroll
+  for (int sp = 7; sp >= 4; --sp) {
+    const int s = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+      gs_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+  // Stages LR + s', s' = 3..0: column bit 7-s' == register bit 3-s'.
+#pragma unroll
+  for (int sp = 3; sp >= 0; --sp) {
+    const int s = LR + sp, d = 8 >> sp;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
+      gs_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
+  __syncthreads();
+  store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+}
+
+// ---- small transforms (N <= 2048): one CTA per tower, strict arithmetic -------
+template <bool INV>
+__global__ void __launch_bounds__(kNttThreads) ntt_small(NttBatch b, DeviceTables T) {
+  __shared__ u64 a[2048];
+  const TowerView v = tower_view(b, T, INV);
+  const int logn = T.logn, n = 1 << logn;
+  const u64 q = v.c->q;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = v.src[i];
+  __syncthreads();
+  if (!INV) {
+    for (int s = 0; s < logn; ++s) {
+      const int lt = logn - 1 - s;  // pair distance 2^lt
+      for (int p = threadIdx.x; p < n / 2; p += blockDim.x) {
+        const int grp = p >> lt, j = (grp << (lt + 1)) + (p & ((1 << lt) - 1));
+        const Shoup w = tw_load(v.tw + (1 << s) + grp);
+        const u64 t = shoup_canon(a[j + (1 << lt)], w.w, w.wq, q);
+        const u64 x = a[j];
+        a[j] = add_mod(x, t, q);
+        a[j + (1 << lt)] = sub_mod(x, t, q);
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int s = logn - 1; s >= 0; --s) {
+      const int lt = logn - 1 - s;
+      for (int p = threadIdx.x; p < n / 2; p += blockDim.x) {
+        const int grp = p >> lt, j = (grp << (lt + 1)) + (p & ((1 << lt) - 1));
+        const u64 x = a[j], y = a[j + (1 << lt)];
+        if (s == 0) {
+          a[j] = shoup_canon(add_mod(x, y, q), v.c->ninv.w, v.c->ninv.wq, q);
+          a[j + (1 << lt)] = shoup_canon(sub_mod(x, y, q), v.c->last_inv.w, v.c->last_inv.wq, q);
+        } else {
+          const Shoup w = tw_load(v.tw + (1 << s) + grp);
+          a[j] = add_mod(x, y, q);
+          a[j + (1 << lt)] = shoup_canon(sub_mod(x, y, q), w.w, w.wq, q);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v.dst[i] = a[i];
+}
+
+}  // namespace b200

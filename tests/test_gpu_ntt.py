@@ -1,0 +1,95 @@
+"""GPU parity: forward/inverse NTT through the C ABI against the CPU oracle."""
+import numpy as np
+import pytest
+
+import ntt_gpu_b200 as nb
+from oracle.oracle import LCG_SEED, PINNED_N, PINNED_P, PINNED_P_PSI, PINNED_Q, PINNED_Q_PSI
+
+pytestmark = pytest.mark.gpu
+
+
+def towers_for(orc, n, bits_list):
+    q = []
+    for bits in bits_list:
+        for v in orc.find_primes(n, 8, bits):
+            if v not in q:
+                q.append(v)
+                break
+    return q, [orc.find_psi(v, n) for v in q]
+
+
+@pytest.mark.parametrize("logn", [1, 2, 3, 6, 8, 10, 11, 12, 13, 14, 15, 16])
+def test_ntt_roundtrip_matches_oracle(lib, orc, logn):
+    n = 1 << logn
+    bits = [30, 50, 55, 60] if n >= 64 else [20, 30]
+    q, psi = towers_for(orc, n, bits)
+    ctx = nb.Context(n, q, psi)
+    x = orc.lcg(n, q, LCG_SEED + logn)
+    want_fwd = orc.ntt(x, q, psi)
+    want_inv = orc.ntt(x, q, psi, inverse=True)
+    d = nb.to_device(x)
+    out = nb.empty(x.shape)
+    ids = list(range(len(q)))
+    ctx.ntt(out, d, ids)
+    np.testing.assert_array_equal(nb.to_host(out), want_fwd)
+    np.testing.assert_array_equal(nb.to_host(d), x)  # out-of-place leaves the source intact
+    back = nb.empty(x.shape)
+    ctx.ntt(back, out, ids, inverse=True)
+    np.testing.assert_array_equal(nb.to_host(back), x)
+    ctx.ntt(out, d, ids, inverse=True)
+    np.testing.assert_array_equal(nb.to_host(out), want_inv)
+
+
+@pytest.mark.parametrize("logn", [10, 16])
+def test_ntt_strict_path_for_wide_moduli(lib, orc, logn):
+    """Moduli in [2^62, 2^63) disable lazy reduction; results stay exact."""
+    n = 1 << logn
+    q = orc.find_primes(n, 2, 63)
+    psi = [orc.find_psi(v, n) for v in q]
+    ctx = nb.Context(n, q, psi)
+    x = orc.lcg(n, q, 11)
+    out = nb.empty(x.shape)
+    ctx.ntt(out, nb.to_device(x), [0, 1])
+    np.testing.assert_array_equal(nb.to_host(out), orc.ntt(x, q, psi))
+    back = nb.empty(x.shape)
+    ctx.ntt(back, out, [0, 1], inverse=True)
+    np.testing.assert_array_equal(nb.to_host(back), x)
+
+
+def test_pinned_openfhe_towers_edge_patterns(lib, orc):
+    """The pinned OpenFHE Q/P table at N=65536: zeros, q-1, monomials, random."""
+    mods = PINNED_Q + PINNED_P
+    psis = PINNED_Q_PSI + PINNED_P_PSI
+    n = PINNED_N
+    ctx = nb.Context(n, PINNED_Q, PINNED_Q_PSI, PINNED_P, PINNED_P_PSI, 3)
+    patterns = [np.zeros((len(mods), n), dtype=np.uint64),
+                np.array([[q - 1] * n for q in mods], dtype=np.uint64)]
+    mono = np.zeros((len(mods), n), dtype=np.uint64)
+    for t, deg in enumerate([0, 1, 17, n - 1, 5, 1000, 32768, 65535]):
+        mono[t, deg] = 1
+    patterns += [mono, orc.lcg(n, mods, LCG_SEED)]
+    ids = list(range(len(mods)))
+    for x in patterns:
+        out = nb.empty(x.shape)
+        ctx.ntt(out, nb.to_device(x), ids)
+        np.testing.assert_array_equal(nb.to_host(out), orc.ntt(x, mods, psis))
+        back = nb.empty(x.shape)
+        ctx.ntt(back, out, ids, inverse=True)
+        np.testing.assert_array_equal(nb.to_host(back), x)
+
+
+def test_batched_polys_with_stride(lib, orc):
+    n = 1 << 14
+    q, psi = towers_for(orc, n, [50, 55, 60])
+    ctx = nb.Context(n, q, psi)
+    polys = 5
+    stride = (len(q) + 1) * n
+    buf = np.zeros((polys, len(q) + 1, n), dtype=np.uint64)
+    for p in range(polys):
+        buf[p, :len(q)] = orc.lcg(n, q, 100 + p)
+    d = nb.to_device(buf)
+    ctx.ntt(d, d, list(range(len(q))), polys=polys, poly_stride=stride)
+    got = nb.to_host(d).reshape(buf.shape)
+    for p in range(polys):
+        np.testing.assert_array_equal(got[p, :len(q)], orc.ntt(buf[p, :len(q)], q, psi))
+        np.testing.assert_array_equal(got[p, len(q)], 0)  # the gap tower is untouched
