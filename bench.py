@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark: batched CKKS Hybrid key switching on B200 (sm_100a).
+
+Workload (one step): a batch of 16 ciphertext components at N = 2^16, L = 24
+active Q towers (55-bit), K = 8 P towers (60-bit), dnum = 3 (alpha = 8), one
+shared full-context switching key, through ntt_b200_keyswitch_batch. Inputs are
+resident in HBM; the working set (~3 GB) is far larger than the 126 MB L2, so
+no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own replica of the workload on its
+own GPU (request-level sharding, no collective on the data path); the timed
+region is bracketed by a barrier + synchronize and the MAX over ranks is used.
+--impl reference times the reference's own CPU implementation (oracle/_ref,
+compiled from its sources) on the host cores instead.
+
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "keyswitch/s N=2^16 L=24 dnum=3 served vs plain, p50/p99 ms; NTT HBM GB/s"
+UNIT = "keyswitch/s"
+N, LEVEL, K_P, DNUM, BATCH = 65536, 24, 8, 3, 16
+SEED = 0x7251D9
+WORKLOAD = ("batched Hybrid key switch: 16 ciphertext components per GPU at N=2^16, L=24 (55-bit), "
+            "K=8 (60-bit), dnum=3 (alpha=8), one shared switching key")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="timed batched steps only (no plain/e2e/CPU legs); for profiler launch lists")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---- clocks during the timed region ------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        sm, smax, reasons = [], [], set()
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(self.NAMES, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---- distributed plumbing -----------------------------------------------------------------
+def dist_setup():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_teardown(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---- CPU side: the reference's own implementation -----------------------------------------
+def cpu_context(prm):
+    from oracle.oracle import Context as OrcContext
+    return OrcContext(prm.n, prm.q, prm.q_psi, prm.p, prm.p_psi, prm.alpha)
+
+
+def cpu_impl():
+    from oracle.oracle import Oracle, Reference
+    if Reference.available():
+        return Reference(), "reference"
+    return Oracle(), "port"
+
+
+def cpu_inputs(prm, level):
+    from ntt_gpu_b200.params import uniform_residues
+    x = uniform_residues(prm.n, prm.q[:level], SEED)[0]
+    kb = uniform_residues(prm.n, prm.q + prm.p, SEED + 1, polys=prm.full_digits())
+    ka = uniform_residues(prm.n, prm.q + prm.p, SEED + 2, polys=prm.full_digits())
+    return x, kb, ka
+
+
+def cpu_baseline_single(prm, samples=3):
+    impl, kind = cpu_impl()
+    ctx = cpu_context(prm)
+    x, kb, ka = cpu_inputs(prm, LEVEL)
+    t0 = time.perf_counter()
+    for _ in range(samples):
+        impl.keyswitch(ctx, LEVEL, x, kb, ka)
+    dt = time.perf_counter() - t0
+    return {"value": samples / dt, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{samples} sequential key switches (N=2^16, L=24, dnum=3, K=8), one thread, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference CPU key switch on every host thread."""
+    if rank != 0:
+        return None
+    from concurrent.futures import ThreadPoolExecutor
+
+    from ntt_gpu_b200.params import synthetic_params
+    prm = synthetic_params(N, LEVEL, K_P, DNUM)
+    impl, kind = cpu_impl()
+    ctx = cpu_context(prm)
+    x, kb, ka = cpu_inputs(prm, LEVEL)
+    threads = os.cpu_count() or 1
+    try:
+        import psutil
+        threads = max(1, min(threads, int(psutil.virtual_memory().available // (700 << 20))))
+    except Exception:
+        pass
+
+    def one(_):
+        impl.keyswitch(ctx, LEVEL, x, kb, ka)
+
+    with ThreadPoolExecutor(threads) as pool:
+        t0 = time.perf_counter()
+        list(pool.map(one, range(threads)))  # one warm-up step
+        t_step = time.perf_counter() - t0
+        steps = max(2, min(args.steps, int(150 / max(t_step, 1e-3))))
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            list(pool.map(one, range(threads)))
+        dt = time.perf_counter() - t0
+    value = threads * steps / dt
+    sample = (f"each step = {threads} concurrent key switches (one per host thread) at N=2^16, L=24, "
+              f"dnum=3, K=8; {steps} timed steps of {args.steps} requested (bounded to a few minutes)")
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": steps, "requested_steps": args.steps, "warmup": 1, "ms_per_step": dt * 1000 / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic", "config": {"workload": WORKLOAD.replace("16 ciphertext components per GPU",
+                                                                          f"{threads} ciphertext components"),
+                                            "n": N, "level": LEVEL, "dnum": DNUM, "k": K_P},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---- GPU side ------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local):
+    import torch
+
+    import ntt_gpu_b200 as nb
+    from ntt_gpu_b200.params import synthetic_params, uniform_residues
+
+    device = local
+    torch.cuda.set_device(device)
+    dev = torch.device(f"cuda:{device}")
+    B = args.batch
+    prm = synthetic_params(N, LEVEL, K_P, DNUM)
+    ctx = nb.Context(prm.n, prm.q, prm.q_psi, prm.p, prm.p_psi, prm.alpha, device)
+    ctx.prepare(LEVEL)
+    T = LEVEL + K_P
+    beta = prm.digits(LEVEL)
+    x = uniform_residues(N, prm.q, SEED + 1000 * rank, polys=B)
+    kb = uniform_residues(N, prm.q + prm.p, SEED + 1, polys=prm.full_digits())
+    ka = uniform_residues(N, prm.q + prm.p, SEED + 2, polys=prm.full_digits())
+    d_x, d_kb, d_ka = nb.to_device(x, device), nb.to_device(kb, device), nb.to_device(ka, device)
+    out_b = torch.empty((B, LEVEL, N), dtype=torch.int64, device=dev)
+    out_a = torch.empty_like(out_b)
+    ws = ctx.workspace(nb.OP_KEYSWITCH, LEVEL, B)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.keyswitch_batch(LEVEL, B, out_b, out_a, d_x, d_kb, d_ka, ws, stream=stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region: K batched steps --------------------------------------------------------
+    clocks = ClockSampler(device)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    nb.timing_reset()
+    nb.timing_enable(True)
+    launches0 = nb.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    launches = nb.kernel_launches() - launches0
+    nb.timing_enable(False)
+    clock_info = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    kernels = {}
+    for name in nb.KERNEL_CLASSES:
+        count, total = nb.timing_query(name)
+        if count:
+            kernels[name] = {"launches": count, "total_ms": total, "avg_ms": total / count}
+    nb.timing_reset()
+    value = B * args.steps * world / (ms / 1000.0)
+
+    # ---- roofline: forward NTT (column + row pass), the dominant kernel family ----------------------
+    W = 8 * N
+    fwd_towers_per_step = B * (beta * T - LEVEL + 2 * LEVEL)  # digit complements + both ModDown channels
+    inv_towers_per_step = B * (LEVEL + 2 * K_P)
+    peak, peak_kind = peaks()
+    roof = None
+    if "ntt_fwd_col" in kernels and "ntt_fwd_row" in kernels:
+        fwd_ms = (kernels["ntt_fwd_col"]["total_ms"] + kernels["ntt_fwd_row"]["total_ms"]) / args.steps
+        achieved = fwd_towers_per_step * 2 * W / (fwd_ms / 1000.0) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ntt_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                tr = json.load(f)
+            per_tower = tr.get("ntt_fwd_dram_bytes_per_tower")
+            if per_tower:
+                traffic = per_tower * fwd_towers_per_step / (kernels["ntt_fwd_col"]["launches"] / args.steps)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "ntt_fwd_col + ntt_fwd_row (forward NTT, both passes)",
+                "algorithmic_bytes_per_launch_pair": (fwd_towers_per_step * 2 * W) /
+                (kernels["ntt_fwd_col"]["launches"] / args.steps),
+                "units": "2 x 524288 B (read + write) per tower-transform; "
+                         f"{fwd_towers_per_step} forward tower-transforms per step"}
+    total_kernel_ms = sum(k["total_ms"] for k in kernels.values()) or 1.0
+    for k in kernels.values():
+        k["share"] = k["total_ms"] / total_kernel_ms
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N, "level": LEVEL, "dnum": DNUM, "alpha": prm.alpha, "k": K_P,
+                       "batch_per_gpu": B, "global_batch": B * world,
+                       "parallelism": f"replicas x{world} (request-level sharding, no collective)",
+                       "l2": "inputs, keys, outputs and workspace (~3 GB) exceed the 126 MB L2; no flush"},
+            "gpu_launches": launches, "roofline": roof, "clocks": clock_info, "kernels": kernels,
+            "ntt_towers_per_step": {"forward": fwd_towers_per_step, "inverse": inv_towers_per_step}}
+    if args.kernels_only:
+        ctx.close()
+        return line
+
+    # ---- plain path: one request at a time (per-request latency) -------------------------------------
+    ws1 = ctx.workspace(nb.OP_KEYSWITCH, LEVEL, 1)
+    lat = []
+    torch.cuda.synchronize(dev)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(B)]
+    plain_steps = max(1, min(args.steps, 10))
+    p0.record(stream)
+    for s in range(plain_steps):
+        for r in range(B):
+            if s == plain_steps - 1:
+                per[r][0].record(stream)
+            ctx.keyswitch(LEVEL, out_b[r], out_a[r], d_x[r], d_kb, d_ka, ws1, stream=stream)
+            if s == plain_steps - 1:
+                per[r][1].record(stream)
+    p1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = max_over_ranks(p0.elapsed_time(p1), world, dev)
+    lat = sorted(a.elapsed_time(b) for a, b in per)
+    plain = {"value": B * plain_steps * world / (plain_ms / 1000.0), "unit": UNIT,
+             "latency_p50_ms": statistics.median(lat),
+             "latency_p99_ms": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
+             "note": "same kernels, one request per call, back to back on one stream"}
+
+    # ---- end to end through the public API with host buffers -----------------------------------------
+    h_x = torch.from_numpy(x.view("int64")).pin_memory()
+    h_b = torch.empty((B, LEVEL, N), dtype=torch.int64).pin_memory()
+    h_a = torch.empty_like(h_b).pin_memory()
+    e2e_steps = max(1, min(args.steps, 10))
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(e2e_steps):
+        d_x.copy_(h_x, non_blocking=True)
+        step()
+        h_b.copy_(out_b, non_blocking=True)
+        h_a.copy_(out_a, non_blocking=True)
+    q1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1), world, dev)
+    e2e = {"value": B * e2e_steps * world / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": int(h_x.numel() * 8), "d2h_bytes_per_step": int((h_b.numel() + h_a.numel()) * 8),
+           "steps": e2e_steps}
+
+    line["e2e"] = e2e
+    line["plain"] = plain
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_single(prm)
+    ctx.close()
+    return line
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # Rank 0 alone times the CPU reference; other ranks exit without work.
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, rank, int(os.environ.get("WORLD_SIZE", "1")))
+    else:
+        rank, world, local = dist_setup()
+        try:
+            line = run_ours(args, rank, world, local)
+        finally:
+            dist_teardown(world)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

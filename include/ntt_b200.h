@@ -147,6 +147,27 @@ int ntt_b200_keyswitch(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint
                        const uint64_t *c0, uint32_t automorphism, void *workspace,
                        size_t workspace_bytes, void *stream);
 
+/* Batched key switch: `batch` evaluation-Q_L components src[batch][L][N] at one
+ * level with one shared full-context key; outputs out_b/out_a[batch][L][N];
+ * c0 (optional) is [batch][L][N] and every request rotates by the same
+ * automorphism. Each launch of the pipeline covers the whole batch. The
+ * reference has no batch API; per request this equals ntt_b200_keyswitch. */
+int ntt_b200_keyswitch_batch(ntt_b200_context ctx, size_t level, size_t batch, uint64_t *out_b,
+                             uint64_t *out_a, const uint64_t *src, const uint64_t *key_b,
+                             const uint64_t *key_a, const uint64_t *c0, uint32_t automorphism,
+                             void *workspace, size_t workspace_bytes, void *stream);
+
+/* Opt-in per-kernel timing: while enabled, every launch of this library is
+ * bracketed by CUDA events on its own stream. query() waits for the recorded
+ * events and returns the launch count and summed device time of one kernel
+ * class ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col",
+ * "ntt_small", "conv", "mac", "rotate", "correct", "pointwise"). The external
+ * clock protocol mirrors the reference's collect_elapsed
+ * (include/ntt/measurement.hpp:41-58). */
+int ntt_b200_timing_enable(int on);
+int ntt_b200_timing_reset(void);
+int ntt_b200_timing_query(const char *kernel, uint64_t *launches, double *total_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,10 @@ _SIGNATURES = {
     "ntt_b200_mod_down": ([_P, _SZ, _P, _P, _P, _SZ, _P], _I),
     "ntt_b200_hybrid_digits": ([_P, _SZ, _P, _P, _P, _SZ, _P], _I),
     "ntt_b200_keyswitch": ([_P, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
+    "ntt_b200_keyswitch_batch": ([_P, _SZ, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
+    "ntt_b200_timing_enable": ([_I], _I),
+    "ntt_b200_timing_reset": ([], _I),
+    "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),
 }
 
 
@@ -219,11 +223,36 @@ class Context:
         _check(self._lib.ntt_b200_hybrid_digits(self._h, level, _ptr(digits), _ptr(src), _ptr(workspace),
                                                 workspace.numel() * 8, _stream(stream)))
 
+    def keyswitch_batch(self, level, batch, out_b, out_a, src, key_b, key_a, workspace, c0=None,
+                        automorphism=0, stream=None):
+        _check(self._lib.ntt_b200_keyswitch_batch(self._h, level, batch, _ptr(out_b), _ptr(out_a), _ptr(src),
+                                                  _ptr(key_b), _ptr(key_a), _ptr(c0), automorphism,
+                                                  _ptr(workspace), workspace.numel() * 8, _stream(stream)))
+
     def keyswitch(self, level, out_b, out_a, src, key_b, key_a, workspace, c0=None, automorphism=0,
                   stream=None):
         _check(self._lib.ntt_b200_keyswitch(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(src), _ptr(key_b),
                                             _ptr(key_a), _ptr(c0), automorphism, _ptr(workspace),
                                             workspace.numel() * 8, _stream(stream)))
+
+
+KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col", "ntt_small", "conv", "mac",
+                  "rotate", "correct", "pointwise")
+
+
+def timing_enable(on: bool = True):
+    _check(load().ntt_b200_timing_enable(int(on)))
+
+
+def timing_reset():
+    _check(load().ntt_b200_timing_reset())
+
+
+def timing_query(kernel: str):
+    """(launches, total device milliseconds) of one kernel class since the last reset."""
+    n, ms = _U64(), ctypes.c_double()
+    _check(load().ntt_b200_timing_query(kernel.encode(), ctypes.byref(n), ctypes.byref(ms)))
+    return int(n.value), float(ms.value)
 
 
 def to_device(array, device=0):

@@ -254,10 +254,51 @@ void require_aligned(std::initializer_list<const void *> ptrs) {
             "device pointers must be 16-byte aligned");
 }
 
-void after_launch(int count = 1) {
-  CUDA_CHECK(cudaGetLastError());
-  g_launches += count;
-}
+// ---- per-kernel CUDA-event timing (opt-in) ------------------------------------------
+// When enabled, every launch is bracketed by two events on its own stream; the
+// query sums cudaEventElapsedTime per kernel class (the external-clock protocol
+// of the reference's collect_elapsed, include/ntt/measurement.hpp:41-58).
+struct TimerRecord {
+  const char *name;
+  cudaEvent_t start, stop;
+};
+struct TimerRegistry {
+  std::mutex mu;
+  std::atomic<bool> enabled{false};
+  std::vector<TimerRecord> records;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t take() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    CUDA_CHECK(cudaEventCreate(&e));
+    return e;
+  }
+} g_timer;
+
+struct Timed {
+  const char *name;
+  cudaStream_t st;
+  cudaEvent_t start = nullptr;
+  Timed(const char *kernel, cudaStream_t stream) : name(kernel), st(stream) {
+    if (!g_timer.enabled.load()) return;
+    std::lock_guard<std::mutex> lock(g_timer.mu);
+    start = g_timer.take();
+    CUDA_CHECK(cudaEventRecord(start, st));
+  }
+  void done() {
+    CUDA_CHECK(cudaGetLastError());
+    g_launches += 1;
+    if (!start) return;
+    std::lock_guard<std::mutex> lock(g_timer.mu);
+    cudaEvent_t stop = g_timer.take();
+    CUDA_CHECK(cudaEventRecord(stop, st));
+    g_timer.records.push_back({name, start, stop});
+  }
+};
 
 // ---- NTT launches ----------------------------------------------------------------
 struct Slot {
@@ -265,47 +306,79 @@ struct Slot {
   uint16_t id;
 };
 
+// Where the second pass of a forward transform writes, when it differs from
+// the first pass's output: a split (b/a) destination and the ModDown epilogue.
+struct NttFinal {
+  u64 *dst = nullptr, *dst_odd = nullptr;
+  u64 stride = 0;
+  const u64 *epi_left = nullptr;
+  u64 epi_left_stride = 0;
+  const b200::Shoup *epi_pinv = nullptr;
+};
+
 template <int LOGN, bool LAZY>
-void launch_ntt_2pass(const Ctx &c, u64 *dst, const u64 *src, const b200::NttBatch &b, int slots,
-                      int polys, bool inverse, cudaStream_t st) {
+void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
+                      bool inverse, cudaStream_t st) {
   const dim3 grid((1u << LOGN) / b200::kTileWords, slots, polys);
-  b200::NttBatch first = b;
-  first.src = src;
-  first.dst = dst;
   b200::NttBatch second = b;
-  second.src = dst;
-  second.dst = dst;
-  if (!inverse) {
-    b200::ntt_fwd_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(first, c.tables);
-    b200::ntt_fwd_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
-  } else {
-    b200::ntt_inv_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(first, c.tables);
-    b200::ntt_inv_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+  second.src = b.dst;
+  second.src_stride = b.dst_stride;
+  if (fin) {
+    second.dst = fin->dst;
+    second.dst_odd = fin->dst_odd;
+    second.dst_stride = fin->stride;
+    second.epi_left = fin->epi_left;
+    second.epi_left_stride = fin->epi_left_stride;
+    second.epi_pinv = fin->epi_pinv;
   }
-  after_launch(2);
+  if (!inverse) {
+    Timed t1("ntt_fwd_col", st);
+    b200::ntt_fwd_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
+    t1.done();
+    Timed t2("ntt_fwd_row", st);
+    b200::ntt_fwd_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+    t2.done();
+  } else {
+    Timed t1("ntt_inv_row", st);
+    b200::ntt_inv_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
+    t1.done();
+    Timed t2("ntt_inv_col", st);
+    b200::ntt_inv_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+    t2.done();
+  }
 }
 
 template <bool LAZY>
-void launch_ntt_chunk(const Ctx &c, u64 *dst, const u64 *src, const b200::NttBatch &b, int slots,
-                      int polys, bool inverse, cudaStream_t st) {
+void launch_ntt_chunk(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
+                      bool inverse, cudaStream_t st) {
   switch (c.logn) {
-    case 12: launch_ntt_2pass<12, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
-    case 13: launch_ntt_2pass<13, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
-    case 14: launch_ntt_2pass<14, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
-    case 15: launch_ntt_2pass<15, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
-    case 16: launch_ntt_2pass<16, LAZY>(c, dst, src, b, slots, polys, inverse, st); break;
+    case 12: launch_ntt_2pass<12, LAZY>(c, b, fin, slots, polys, inverse, st); break;
+    case 13: launch_ntt_2pass<13, LAZY>(c, b, fin, slots, polys, inverse, st); break;
+    case 14: launch_ntt_2pass<14, LAZY>(c, b, fin, slots, polys, inverse, st); break;
+    case 15: launch_ntt_2pass<15, LAZY>(c, b, fin, slots, polys, inverse, st); break;
+    case 16: launch_ntt_2pass<16, LAZY>(c, b, fin, slots, polys, inverse, st); break;
     default: throw ContractError("unsupported ring dimension");
   }
 }
 
-// NTT of a list of slots; each slot is (tower offset from base, global id).
+dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
+  return dim3((unsigned)((c.n + b200::kEwThreads - 1) / b200::kEwThreads), (unsigned)towers,
+              (unsigned)polys);
+}
+
+// NTT of a list of slots (tower offset from the base, global id) over `polys`
+// polynomials with separate source and destination strides (words). `fin`
+// (forward only) redirects the final pass: split destination and/or the ModDown
+// epilogue (left - x) * P^-1; small transforms run it as a separate kernel.
 void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots, size_t polys,
-             u64 poly_stride, bool inverse, cudaStream_t st) {
+             u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
+  require(!fin || !inverse, "final-pass redirection is forward only");
   for (size_t first = 0; first < slots.size(); first += b200::kMaxSlots) {
     const size_t count = std::min<size_t>(b200::kMaxSlots, slots.size() - first);
     b200::NttBatch b{};
-    b.poly_stride = poly_stride;
+    b.src_stride = src_stride;
+    b.dst_stride = dst_stride;
     for (size_t i = 0; i < count; ++i) {
       b.off[i] = slots[first + i].off;
       b.id[i] = slots[first + i].id;
@@ -315,15 +388,36 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
     if (c.logn <= 11) {
       const dim3 grid(1, (unsigned)count, (unsigned)polys);
       const int threads = std::min<int>(b200::kNttThreads, std::max<int>(32, (int)(c.n / 2)));
-      if (inverse)
-        b200::ntt_small<true><<<grid, threads, 0, st>>>(b, c.tables);
-      else
-        b200::ntt_small<false><<<grid, threads, 0, st>>>(b, c.tables);
-      after_launch();
+      {
+        Timed t("ntt_small", st);
+        if (inverse)
+          b200::ntt_small<true><<<grid, threads, 0, st>>>(b, c.tables);
+        else
+          b200::ntt_small<false><<<grid, threads, 0, st>>>(b, c.tables);
+        t.done();
+      }
+      if (fin) {
+        // Separate tail: only contiguous Q-slot layouts (slot i = Q tower i) reach here.
+        b200::CorrectArgs a{};
+        a.dst = fin->dst;
+        a.dst_odd = fin->dst_odd;
+        a.left = fin->epi_left;
+        a.right = dst;
+        a.pinv = fin->epi_pinv;
+        a.tc = c.d_tc;
+        a.poly_stride_dst = fin->stride;
+        a.poly_stride_left = fin->epi_left_stride;
+        a.poly_stride_right = dst_stride;
+        a.towers = (int)count;
+        a.logn = c.logn;
+        Timed t("correct", st);
+        b200::correct_kernel<<<ew_grid(c, count, polys), b200::kEwThreads, 0, st>>>(a);
+        t.done();
+      }
     } else if (c.lazy) {
-      launch_ntt_chunk<true>(c, dst, src, b, (int)count, (int)polys, inverse, st);
+      launch_ntt_chunk<true>(c, b, fin, (int)count, (int)polys, inverse, st);
     } else {
-      launch_ntt_chunk<false>(c, dst, src, b, (int)count, (int)polys, inverse, st);
+      launch_ntt_chunk<false>(c, b, fin, (int)count, (int)polys, inverse, st);
     }
   }
 }
@@ -355,6 +449,7 @@ void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, cu
 void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
               const std::vector<uint16_t> &slots, size_t polys, u64 src_stride, u64 dst_stride,
               cudaStream_t st) {
+  require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   b200::ConvArgs a{};
   a.plan = p.device;
   a.src = src;
@@ -363,87 +458,102 @@ void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
   a.dst_poly_stride = dst_stride;
   for (size_t i = 0; i < slots.size(); ++i) a.slot[i] = slots[i];
   a.logn = c.logn;
-  a.targets_per_block = 8;
+  // All targets per block when the batch alone fills the GPU (the scaled
+  // inputs y_j are then computed once per coefficient); otherwise split the
+  // targets across blocks for parallelism.
+  const size_t base_blocks = ((c.n + b200::kEwThreads - 1) / b200::kEwThreads) * polys;
+  const size_t want_blocks = 148 * 8;
+  int tpb = p.t;
+  if (base_blocks < want_blocks) tpb = std::max<int>(4, (int)((p.t * base_blocks + want_blocks - 1) / want_blocks));
+  a.targets_per_block = std::min(tpb, p.t);
   const dim3 grid((unsigned)((c.n + b200::kEwThreads - 1) / b200::kEwThreads),
                   (unsigned)((p.t + a.targets_per_block - 1) / a.targets_per_block), (unsigned)polys);
+  Timed t("conv", st);
   if (p.s <= 4) launch_conv_t<4>(p, a, grid, st);
   else if (p.s <= 8) launch_conv_t<8>(p, a, grid, st);
   else if (p.s <= 16) launch_conv_t<16>(p, a, grid, st);
   else launch_conv_t<40>(p, a, grid, st);
-  after_launch();
-}
-
-dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
-  return dim3((unsigned)((c.n + b200::kEwThreads - 1) / b200::kEwThreads), (unsigned)towers,
-              (unsigned)polys);
+  t.done();
 }
 
 // ---- workspace carving -----------------------------------------------------------
+size_t aligned_bytes(size_t words) { return ((words * sizeof(u64)) + 255) / 256 * 256; }
 struct Carver {
   char *base;
   size_t size, used = 0;
   u64 *take(size_t words) {
-    const size_t bytes = ((words * sizeof(u64)) + 255) / 256 * 256;
+    const size_t bytes = aligned_bytes(words);
     if (used + bytes > size) throw WorkspaceError("workspace too small");
     u64 *p = reinterpret_cast<u64 *>(base + used);
     used += bytes;
     return p;
   }
 };
-size_t aligned_words(size_t words) { return ((words * sizeof(u64)) + 255) / 256 * 256; }
 
 size_t workspace_bytes(const Ctx &c, int op, size_t level, size_t batch) {
-  const size_t n = c.n, L = level, K = c.k, T = L + K;
+  const size_t n = c.n, L = level, K = c.k, T = L + K, B = batch;
   const size_t beta = 1 + (L - 1) / c.alpha;
-  size_t bytes = 0;
   switch (op) {
-    case NTT_B200_OP_MOD_UP: bytes = aligned_words(L * n); break;
-    case NTT_B200_OP_MOD_DOWN: bytes = aligned_words(K * n) + aligned_words(L * n); break;
-    case NTT_B200_OP_DIGITS: bytes = aligned_words(L * n); break;
+    case NTT_B200_OP_MOD_UP: return aligned_bytes(B * L * n);
+    case NTT_B200_OP_MOD_DOWN: return aligned_bytes(B * K * n) + aligned_bytes(B * L * n);
+    case NTT_B200_OP_DIGITS: return aligned_bytes(B * L * n);
     case NTT_B200_OP_KEYSWITCH:
-      bytes = aligned_words(beta * T * n) + aligned_words(L * n) + 2 * aligned_words(T * n) +
-              2 * aligned_words(T * n) + aligned_words(K * n) + aligned_words(L * n);
-      break;
+      return aligned_bytes(B * beta * T * n) + aligned_bytes(B * L * n) + 2 * aligned_bytes(2 * B * T * n) +
+             aligned_bytes(2 * B * K * n) + aligned_bytes(2 * B * L * n);
     default: throw ContractError("unknown workspace operation");
   }
-  return bytes * batch;
 }
 
-// ---- composite operations (one request) -------------------------------------------
-void do_mod_down(Ctx &c, size_t L, u64 *dst, const u64 *src, Carver &ws, cudaStream_t st) {
+Carver carve(const Ctx &c, void *ws, size_t bytes, int op, size_t level, size_t batch) {
+  const size_t need = workspace_bytes(c, op, level, batch);
+  if (need && (!ws || bytes < need)) throw WorkspaceError("workspace missing or too small");
+  return Carver{reinterpret_cast<char *>(ws), bytes};
+}
+
+// ---- composite operations over a batch of polynomials ----------------------------------
+// ModDown of `polys` evaluation-QP polynomials (stride src_stride) into
+// evaluation Q_L (stride dst_stride, or split even/odd destinations).
+void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst_stride, const u64 *src,
+                 u64 src_stride, Carver &ws, cudaStream_t st) {
   const size_t n = c.n, K = c.k;
-  u64 *p_coeff = ws.take(K * n);
-  u64 *corr = ws.take(L * n);
-  run_ntt(c, p_coeff, src + L * n, contiguous_slots(range_ids(c.m, c.m + K)), 1, 0, true, st);
+  u64 *p_coeff = ws.take(polys * K * n);
+  u64 *corr = ws.take(polys * L * n);
+  run_ntt(c, p_coeff, src + L * n, contiguous_slots(range_ids(c.m, c.m + K)), polys, src_stride, K * n,
+          true, st);
   const auto &plan = c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L));
   std::vector<uint16_t> slots;
   for (size_t i = 0; i < L; ++i) slots.push_back((uint16_t)i);
-  run_conv(c, plan, corr, p_coeff, slots, 1, 0, 0, st);
-  run_ntt(c, corr, corr, contiguous_slots(range_ids(0, L)), 1, 0, false, st);
-  b200::CorrectArgs a{};
-  a.dst = dst;
-  a.left = src;
-  a.right = corr;
-  a.plan = c.down_plan(L);
-  a.tc = c.d_tc;
-  a.towers = (int)L;
-  a.logn = c.logn;
-  b200::correct_kernel<<<ew_grid(c, L, 1), b200::kEwThreads, 0, st>>>(a);
-  after_launch();
+  run_conv(c, plan, corr, p_coeff, slots, polys, K * n, L * n, st);
+  NttFinal fin;
+  fin.dst = dst;
+  fin.dst_odd = dst_odd;
+  fin.stride = dst_stride;
+  fin.epi_left = src;
+  fin.epi_left_stride = src_stride;
+  fin.epi_pinv = c.down_plan(L)->p_inv;
+  run_ntt(c, corr, corr, contiguous_slots(range_ids(0, L)), polys, L * n, L * n, false, st, &fin);
 }
 
-void do_digits(Ctx &c, size_t L, u64 *digits, const u64 *src, Carver &ws, cudaStream_t st) {
+// Hybrid digits of `polys` evaluation-Q_L inputs (stride L*n) into digits
+// (stride beta*T*n). copy_own = false leaves each digit's own towers unwritten
+// (the fused MAC reads them from the input).
+void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carver &ws, bool copy_own,
+               cudaStream_t st) {
   const size_t n = c.n, K = c.k, T = L + K;
-  u64 *coeff = ws.take(L * n);
-  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), 1, 0, true, st);
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  const u64 dstride = beta * T * n;
+  u64 *coeff = ws.take(polys * L * n);
+  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), polys, L * n, L * n, true, st);
   const auto all = qp_ids(c, L);
   std::vector<Slot> fwd;
   size_t digit = 0;
   for (size_t first = 0; first < L; first += c.alpha, ++digit) {
     const size_t count = std::min(c.alpha, L - first);
     u64 *out = digits + digit * T * n;
-    CUDA_CHECK(cudaMemcpyAsync(out + first * n, src + first * n, count * n * sizeof(u64),
-                               cudaMemcpyDeviceToDevice, st));
+    if (copy_own)
+      CUDA_CHECK(cudaMemcpy2DAsync(out + first * n, dstride * sizeof(u64), src + first * n,
+                                   L * n * sizeof(u64), count * n * sizeof(u64), polys,
+                                   cudaMemcpyDeviceToDevice, st));
     std::vector<uint16_t> tgt, slots;
     for (size_t t = 0; t < T; ++t)
       if (t < first || t >= first + count) {
@@ -452,41 +562,49 @@ void do_digits(Ctx &c, size_t L, u64 *digits, const u64 *src, Carver &ws, cudaSt
         fwd.push_back({(uint32_t)(digit * T + t), all[t]});
       }
     const auto &plan = c.conv_plan(range_ids(first, first + count), tgt);
-    run_conv(c, plan, out, coeff + first * n, slots, 1, 0, 0, st);
+    run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st);
   }
-  run_ntt(c, digits, digits, fwd, 1, 0, false, st);
+  run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st);
 }
 
-void do_mac(Ctx &c, size_t L, u64 *out_b, u64 *out_a, const u64 *digits, const u64 *key_b,
-            const u64 *key_a, cudaStream_t st) {
+// MAC of `polys` requests: out_b/out_a of request z at out + z * out_stride.
+void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride, const u64 *digits,
+            const u64 *input, const u64 *key_b, const u64 *key_a, cudaStream_t st) {
   const size_t n = c.n, T = L + c.k;
   const size_t beta = 1 + (L - 1) / c.alpha;
   b200::MacArgs a{};
   a.out_b = out_b;
   a.out_a = out_a;
   a.digits = digits;
+  a.input = input;
   a.key_b = key_b;
   a.key_a = key_a;
   a.tc = c.d_tc;
   a.digit_stride = T * n;
   a.key_digit_stride = c.towers() * n;
+  a.poly_stride_out = out_stride;
+  a.poly_stride_digits = beta * T * n;
+  a.poly_stride_input = L * n;
   a.level = (int)L;
   a.m = (int)c.m;
   a.beta = (int)beta;
+  a.alpha = (int)c.alpha;
   a.logn = c.logn;
   u64 max_q = 0;
   for (auto q : c.mod) max_q = std::max(max_q, q);
   const u128 prod = (u128)(max_q - 1) * (max_q - 1);
   const bool wide = prod > (~(u128)0) / (u128)beta;
+  const dim3 grid((unsigned)((n + b200::kEwThreads - 1) / b200::kEwThreads), (unsigned)polys, (unsigned)T);
+  Timed t("mac", st);
   if (wide)
-    b200::mac_kernel<true><<<ew_grid(c, T, 1), b200::kEwThreads, 0, st>>>(a);
+    b200::mac_kernel<true><<<grid, b200::kEwThreads, 0, st>>>(a);
   else
-    b200::mac_kernel<false><<<ew_grid(c, T, 1), b200::kEwThreads, 0, st>>>(a);
-  after_launch();
+    b200::mac_kernel<false><<<grid, b200::kEwThreads, 0, st>>>(a);
+  t.done();
 }
 
-void do_rotate(Ctx &c, size_t L, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,
-               const u64 *c0, uint32_t g, cudaStream_t st) {
+void do_rotate(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,
+               u64 stride, const u64 *c0, u64 c0_stride, uint32_t g, cudaStream_t st) {
   require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
   b200::RotateArgs a{};
   a.out_b = out_b;
@@ -496,18 +614,34 @@ void do_rotate(Ctx &c, size_t L, u64 *out_b, u64 *out_a, const u64 *ext_b, const
   a.c0 = c0;
   a.plan = c.down_plan(L);
   a.tc = c.d_tc;
+  a.poly_stride = stride;
+  a.c0_poly_stride = c0_stride;
   a.level = (int)L;
   a.m = (int)c.m;
   a.logn = c.logn;
   a.g = g;
-  b200::rotate_kernel<<<ew_grid(c, L + c.k, 1), b200::kEwThreads, 0, st>>>(a);
-  after_launch();
+  Timed t("rotate", st);
+  b200::rotate_kernel<<<ew_grid(c, L + c.k, polys), b200::kEwThreads, 0, st>>>(a);
+  t.done();
 }
 
-Carver carve(const Ctx &c, void *ws, size_t bytes, int op, size_t level) {
-  const size_t need = workspace_bytes(c, op, level, 1);
-  if (need && (!ws || bytes < need)) throw WorkspaceError("workspace missing or too small");
-  return Carver{reinterpret_cast<char *>(ws), bytes};
+// The Hybrid key switch of `batch` requests at one level with one shared key:
+// src/out_b/out_a/c0 are [batch][L][N].
+void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const u64 *src, const u64 *key_b,
+                  const u64 *key_a, const u64 *c0, uint32_t g, Carver &ws, cudaStream_t st) {
+  const size_t n = c.n, T = L + c.k;
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  u64 *digits = ws.take(batch * beta * T * n);
+  u64 *acc = ws.take(2 * batch * T * n);  // [batch][b|a][T][N]
+  u64 *rot = ws.take(2 * batch * T * n);
+  do_digits(c, L, batch, digits, src, ws, false, st);
+  do_mac(c, L, batch, acc, acc + T * n, 2 * T * n, digits, src, key_b, key_a, st);
+  const u64 *ext = acc;
+  if (c0) {
+    do_rotate(c, L, batch, rot, rot + T * n, acc, acc + T * n, 2 * T * n, c0, L * n, g, st);
+    ext = rot;
+  }
+  do_mod_down(c, L, 2 * batch, out_b, out_a, L * n, ext, T * n, ws, st);
 }
 }  // namespace
 
@@ -516,6 +650,40 @@ extern "C" {
 
 const char *ntt_b200_last_error(void) { return g_last_error.c_str(); }
 uint64_t ntt_b200_kernel_launches(void) { return g_launches.load(); }
+
+int ntt_b200_timing_enable(int on) {
+  return guarded([&] { g_timer.enabled = on != 0; });
+}
+
+int ntt_b200_timing_reset(void) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(g_timer.mu);
+    for (auto &r : g_timer.records) {
+      g_timer.pool.push_back(r.start);
+      g_timer.pool.push_back(r.stop);
+    }
+    g_timer.records.clear();
+  });
+}
+
+int ntt_b200_timing_query(const char *kernel, uint64_t *launches, double *total_ms) {
+  return guarded([&] {
+    require(kernel && launches && total_ms, "null argument");
+    std::lock_guard<std::mutex> lock(g_timer.mu);
+    uint64_t count = 0;
+    double ms = 0;
+    for (auto &r : g_timer.records) {
+      if (std::strcmp(r.name, kernel) != 0) continue;
+      CUDA_CHECK(cudaEventSynchronize(r.stop));
+      float e = 0;
+      CUDA_CHECK(cudaEventElapsedTime(&e, r.start, r.stop));
+      ms += e;
+      ++count;
+    }
+    *launches = count;
+    *total_ms = ms;
+  });
+}
 
 int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const uint64_t *q,
                             const uint64_t *q_psi, size_t m, const uint64_t *p,
@@ -639,7 +807,7 @@ int ntt_b200_ntt(ntt_b200_context ctx, uint64_t *dst, const uint64_t *src, const
       slots.push_back({(uint32_t)i, (uint16_t)tower_ids[i]});
     }
     DeviceGuard guard(ctx->device);
-    run_ntt(*ctx, dst, src, slots, polys, poly_stride, inverse != 0, as_stream(stream));
+    run_ntt(*ctx, dst, src, slots, polys, poly_stride, poly_stride, inverse != 0, as_stream(stream));
   });
 }
 
@@ -667,8 +835,10 @@ int ntt_b200_pointwise(ntt_b200_context ctx, uint64_t *dst, const uint64_t *left
     a.towers = (int)towers;
     a.logn = ctx->logn;
     DeviceGuard guard(ctx->device);
-    b200::pointwise_kernel<<<ew_grid(*ctx, towers, polys), b200::kEwThreads, 0, as_stream(stream)>>>(a);
-    after_launch();
+    const cudaStream_t st = as_stream(stream);
+    Timed t("pointwise", st);
+    b200::pointwise_kernel<<<ew_grid(*ctx, towers, polys), b200::kEwThreads, 0, st>>>(a);
+    t.done();
   });
 }
 
@@ -708,12 +878,14 @@ int ntt_b200_correct(ntt_b200_context ctx, size_t level, uint64_t *dst, const ui
     a.dst = dst;
     a.left = left;
     a.right = right;
-    a.plan = ctx->down_plan(level);
+    a.pinv = ctx->down_plan(level)->p_inv;
     a.tc = ctx->d_tc;
     a.towers = (int)level;
     a.logn = ctx->logn;
-    b200::correct_kernel<<<ew_grid(*ctx, level, 1), b200::kEwThreads, 0, as_stream(stream)>>>(a);
-    after_launch();
+    const cudaStream_t st = as_stream(stream);
+    Timed t("correct", st);
+    b200::correct_kernel<<<ew_grid(*ctx, level, 1), b200::kEwThreads, 0, st>>>(a);
+    t.done();
   });
 }
 
@@ -726,7 +898,7 @@ int ntt_b200_hybrid_mac(ntt_b200_context ctx, size_t level, uint64_t *out_b, uin
     require(out_b && out_a && digits && key_b && key_a, "null pointer");
     require_aligned({out_b, out_a, digits, key_b, key_a});
     DeviceGuard guard(ctx->device);
-    do_mac(*ctx, level, out_b, out_a, digits, key_b, key_a, as_stream(stream));
+    do_mac(*ctx, level, 1, out_b, out_a, 0, digits, nullptr, key_b, key_a, as_stream(stream));
   });
 }
 
@@ -739,7 +911,7 @@ int ntt_b200_hybrid_rotate(ntt_b200_context ctx, size_t level, uint64_t *out_b, 
     require(out_b && out_a && ext_b && ext_a && c0, "null pointer");
     require_aligned({out_b, out_a, ext_b, ext_a, c0});
     DeviceGuard guard(ctx->device);
-    do_rotate(*ctx, level, out_b, out_a, ext_b, ext_a, c0, automorphism, as_stream(stream));
+    do_rotate(*ctx, level, 1, out_b, out_a, ext_b, ext_a, 0, c0, 0, automorphism, as_stream(stream));
   });
 }
 
@@ -747,7 +919,7 @@ int ntt_b200_workspace_bytes(ntt_b200_context ctx, int op, size_t level, size_t 
   return guarded([&] {
     require_ctx(ctx);
     require_level(ctx, level);
-    require(out != nullptr && batch >= 1, "invalid workspace query");
+    require(out != nullptr && batch >= 1 && batch <= 65535 / 2, "invalid workspace query");
     *out = workspace_bytes(*ctx, op, level, batch);
   });
 }
@@ -760,24 +932,24 @@ int ntt_b200_mod_up(ntt_b200_context ctx, size_t level, uint64_t *dst, const uin
     require(dst && src, "null pointer");
     require_aligned({dst, src, workspace});
     Ctx &c = *ctx;
-    Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_MOD_UP, level);
+    Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_MOD_UP, level, 1);
     DeviceGuard guard(c.device);
     const cudaStream_t st = as_stream(stream);
     const size_t n = c.n, L = level, K = c.k;
     const u64 *coeff = src;
     if (src_is_eval) {
       u64 *tmp = ws.take(L * n);
-      run_ntt(c, tmp, src, contiguous_slots(range_ids(0, L)), 1, 0, true, st);
+      run_ntt(c, tmp, src, contiguous_slots(range_ids(0, L)), 1, 0, 0, true, st);
       CUDA_CHECK(cudaMemcpyAsync(dst, src, L * n * sizeof(u64), cudaMemcpyDeviceToDevice, st));
       coeff = tmp;
     } else {
-      run_ntt(c, dst, src, contiguous_slots(range_ids(0, L)), 1, 0, false, st);
+      run_ntt(c, dst, src, contiguous_slots(range_ids(0, L)), 1, 0, 0, false, st);
     }
     const auto &plan = c.conv_plan(range_ids(0, L), range_ids(c.m, c.m + K));
     std::vector<uint16_t> slots;
     for (size_t i = 0; i < K; ++i) slots.push_back((uint16_t)(L + i));
     run_conv(c, plan, dst, coeff, slots, 1, 0, 0, st);
-    run_ntt(c, dst, dst, contiguous_slots(range_ids(c.m, c.m + K), (uint32_t)L), 1, 0, false, st);
+    run_ntt(c, dst, dst, contiguous_slots(range_ids(c.m, c.m + K), (uint32_t)L), 1, 0, 0, false, st);
   });
 }
 
@@ -788,9 +960,9 @@ int ntt_b200_mod_down(ntt_b200_context ctx, size_t level, uint64_t *dst, const u
     require_level(ctx, level);
     require(dst && src, "null pointer");
     require_aligned({dst, src, workspace});
-    Carver ws = carve(*ctx, workspace, workspace_bytes, NTT_B200_OP_MOD_DOWN, level);
+    Carver ws = carve(*ctx, workspace, workspace_bytes, NTT_B200_OP_MOD_DOWN, level, 1);
     DeviceGuard guard(ctx->device);
-    do_mod_down(*ctx, level, dst, src, ws, as_stream(stream));
+    do_mod_down(*ctx, level, 1, dst, nullptr, 0, src, 0, ws, as_stream(stream));
   });
 }
 
@@ -801,9 +973,9 @@ int ntt_b200_hybrid_digits(ntt_b200_context ctx, size_t level, uint64_t *digits,
     require_level(ctx, level);
     require(digits && src, "null pointer");
     require_aligned({digits, src, workspace});
-    Carver ws = carve(*ctx, workspace, workspace_bytes, NTT_B200_OP_DIGITS, level);
+    Carver ws = carve(*ctx, workspace, workspace_bytes, NTT_B200_OP_DIGITS, level, 1);
     DeviceGuard guard(ctx->device);
-    do_digits(*ctx, level, digits, src, ws, as_stream(stream));
+    do_digits(*ctx, level, 1, digits, src, ws, true, as_stream(stream));
   });
 }
 
@@ -811,34 +983,25 @@ int ntt_b200_keyswitch(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint
                        const uint64_t *src, const uint64_t *key_b, const uint64_t *key_a,
                        const uint64_t *c0, uint32_t automorphism, void *workspace,
                        size_t workspace_bytes, void *stream) {
+  return ntt_b200_keyswitch_batch(ctx, level, 1, out_b, out_a, src, key_b, key_a, c0, automorphism,
+                                  workspace, workspace_bytes, stream);
+}
+
+int ntt_b200_keyswitch_batch(ntt_b200_context ctx, size_t level, size_t batch, uint64_t *out_b,
+                             uint64_t *out_a, const uint64_t *src, const uint64_t *key_b,
+                             const uint64_t *key_a, const uint64_t *c0, uint32_t automorphism,
+                             void *workspace, size_t workspace_bytes, void *stream) {
   return guarded([&] {
     require_ctx(ctx);
     require_level(ctx, level);
+    require(batch >= 1 && batch <= 65535 / 2, "key-switch batch out of range");
     require(out_b && out_a && src && key_b && key_a, "null pointer");
     require_aligned({out_b, out_a, src, key_b, key_a, c0, workspace});
     Ctx &c = *ctx;
     if (c0) require((automorphism & 1) && automorphism < 2 * c.n, "invalid negacyclic automorphism index");
-    Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_KEYSWITCH, level);
+    Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_KEYSWITCH, level, batch);
     DeviceGuard guard(c.device);
-    const cudaStream_t st = as_stream(stream);
-    const size_t n = c.n, L = level, T = L + c.k;
-    const size_t beta = 1 + (L - 1) / c.alpha;
-    u64 *digits = ws.take(beta * T * n);
-    u64 *acc_b = ws.take(T * n);
-    u64 *acc_a = ws.take(T * n);
-    do_digits(c, L, digits, src, ws, st);
-    do_mac(c, L, acc_b, acc_a, digits, key_b, key_a, st);
-    const u64 *ext_b = acc_b, *ext_a = acc_a;
-    if (c0) {
-      u64 *rot_b = ws.take(T * n);
-      u64 *rot_a = ws.take(T * n);
-      do_rotate(c, L, rot_b, rot_a, acc_b, acc_a, c0, automorphism, st);
-      ext_b = rot_b;
-      ext_a = rot_a;
-    }
-    Carver md = ws;
-    do_mod_down(c, L, out_b, ext_b, md, st);
-    do_mod_down(c, L, out_a, ext_a, ws, st);
+    do_keyswitch(c, level, batch, out_b, out_a, src, key_b, key_a, c0, automorphism, ws, as_stream(stream));
   });
 }
 

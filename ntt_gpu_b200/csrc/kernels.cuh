@@ -28,8 +28,8 @@ struct ConvArgs {
 
 template <int MAXS, bool WIDE>
 __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
-  __shared__ u64 hat[MAXS * 16];
-  __shared__ Reducer red[16];
+  __shared__ u64 hat[MAXS * kMaxConvTargets];
+  __shared__ Reducer red[kMaxConvTargets];
   __shared__ u64 sq[MAXS];
   __shared__ Shoup sinv[MAXS];
   const ConvPlan &p = *a.plan;
@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
   const int nt = t1 - t0;
   for (int i = threadIdx.x; i < s * nt; i += blockDim.x) {
     const int j = i / nt, t = i % nt;
-    hat[j * 16 + t] = p.hat[j * p.t + t0 + t];
+    hat[j * nt + t] = p.hat[j * p.t + t0 + t];
   }
   for (int t = threadIdx.x; t < nt; t += blockDim.x) red[t] = p.tgt[t0 + t];
   for (int j = threadIdx.x; j < s; j += blockDim.x) {
@@ -63,13 +63,13 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
       acc_zero(acc);
 #pragma unroll
       for (int j = 0; j < MAXS; ++j)
-        if (j < s) acc_mad(acc, y[j], hat[j * 16 + t]);
+        if (j < s) acc_mad(acc, y[j], hat[j * nt + t]);
       out = reduce(acc, red[t]);
     } else {
       Acc128 acc{0, 0};
 #pragma unroll
       for (int j = 0; j < MAXS; ++j)
-        if (j < s) acc_mad(acc, y[j], hat[j * 16 + t]);
+        if (j < s) acc_mad(acc, y[j], hat[j * nt + t]);
       out = reduce(acc, red[t]);
     }
     dst[u64(a.slot[t0 + t]) * n + k] = out;
@@ -78,9 +78,9 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
 
 // ---- ModDown tail: (l - r) * [P^-1]_q  (resident_conversion.hpp:45-49) ---------
 struct CorrectArgs {
-  u64 *dst;
+  u64 *dst, *dst_odd;  // dst_odd set: polynomial z writes (z odd ? dst_odd : dst) + (z / 2) * stride
   const u64 *left, *right;
-  const DownPlan *plan;
+  const Shoup *pinv;  // [P^-1]_q by Q tower
   const TowerConsts *tc;
   u64 poly_stride_dst, poly_stride_left, poly_stride_right;
   int towers, logn;
@@ -91,11 +91,13 @@ __global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
   const int t = blockIdx.y;
   if (i >= n) return;
   const u64 q = a.tc[t].q;  // Q tower t has global id t
-  const Shoup pinv = a.plan->p_inv[t];
+  const Shoup pinv = a.pinv[t];
   const u64 z = blockIdx.z;
   const u64 l = a.left[z * a.poly_stride_left + t * n + i];
   const u64 r = a.right[z * a.poly_stride_right + t * n + i];
-  a.dst[z * a.poly_stride_dst + t * n + i] = shoup_canon(sub_mod(l, r, q), pinv.w, pinv.wq, q);
+  u64 *dst = a.dst_odd ? ((z & 1) ? a.dst_odd : a.dst) + (z >> 1) * a.poly_stride_dst
+                       : a.dst + z * a.poly_stride_dst;
+  dst[t * n + i] = shoup_canon(sub_mod(l, r, q), pinv.w, pinv.wq, q);
 }
 
 // ---- Hybrid MAC over all digits in one pass --------------------------------------
@@ -106,31 +108,37 @@ __global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
 struct MacArgs {
   u64 *out_b, *out_a;
   const u64 *digits;    // digit d, tower t at digits + d * digit_stride + t * n
+  const u64 *input;     // if set: digit d's own Q towers are read from input + t * n
   const u64 *key_b, *key_a;
   const TowerConsts *tc;
   u64 digit_stride, key_digit_stride;
-  u64 poly_stride_out, poly_stride_digits;
-  int level, m, beta, logn;
+  u64 poly_stride_out, poly_stride_digits, poly_stride_input;
+  int level, m, beta, alpha, logn;
 };
+// Grid: x = coefficient block, y = request, z = QP tower. Requests vary faster
+// than towers, so the key rows of one tower stay in L2 while every request of
+// the batch streams through them.
 template <bool WIDE>
 __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
   const u64 n = u64(1) << a.logn;
   const u64 i = u64(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int t = blockIdx.y;
+  const int t = blockIdx.z;
+  const u64 z = blockIdx.y;
   if (i >= n) return;
   const int g = t < a.level ? t : a.m + (t - a.level);
   const Reducer red = a.tc[g].red;
-  const u64 *d = a.digits + blockIdx.z * a.poly_stride_digits + t * n + i;
+  const u64 *d = a.digits + z * a.poly_stride_digits + t * n + i;
+  const int own = (a.input && t < a.level) ? t / a.alpha : -1;
   const u64 *kb = a.key_b + u64(g) * n + i;
   const u64 *ka = a.key_a + u64(g) * n + i;
   using Acc = typename std::conditional<WIDE, Acc192, Acc128>::type;
   Acc ab{}, aa{};
   for (int j = 0; j < a.beta; ++j) {
-    const u64 x = d[j * a.digit_stride];
+    const u64 x = j == own ? a.input[z * a.poly_stride_input + t * n + i] : d[j * a.digit_stride];
     acc_mad(ab, x, kb[j * a.key_digit_stride]);
     acc_mad(aa, x, ka[j * a.key_digit_stride]);
   }
-  const u64 o = blockIdx.z * a.poly_stride_out + t * n + i;
+  const u64 o = z * a.poly_stride_out + t * n + i;
   a.out_b[o] = reduce(ab, red);
   a.out_a[o] = reduce(aa, red);
 }
@@ -148,6 +156,7 @@ struct RotateArgs {
   const u64 *ext_b, *ext_a, *c0;
   const DownPlan *plan;
   const TowerConsts *tc;
+  u64 poly_stride, c0_poly_stride;
   int level, m, logn;
   uint32_t g;
 };
@@ -156,15 +165,16 @@ __global__ void __launch_bounds__(kEwThreads) rotate_kernel(RotateArgs a) {
   const u64 k = u64(blockIdx.x) * blockDim.x + threadIdx.x;
   const int t = blockIdx.y;
   if (k >= n) return;
+  const u64 z = blockIdx.z;
   const u64 src = t * n + automorphism_source((uint32_t)k, a.logn, a.g);
-  u64 b = a.ext_b[src];
+  u64 b = a.ext_b[z * a.poly_stride + src];
   if (t < a.level) {
     const u64 q = a.tc[t].q;
     const Shoup pm = a.plan->p_mod[t];
-    b = add_mod(b, shoup_canon(a.c0[src], pm.w, pm.wq, q), q);
+    b = add_mod(b, shoup_canon(a.c0[z * a.c0_poly_stride + src], pm.w, pm.wq, q), q);
   }
-  a.out_b[t * n + k] = b;
-  a.out_a[t * n + k] = a.ext_a[src];
+  a.out_b[z * a.poly_stride + t * n + k] = b;
+  a.out_a[z * a.poly_stride + t * n + k] = a.ext_a[z * a.poly_stride + src];
 }
 
 // ---- pointwise product ------------------------------------------------------------

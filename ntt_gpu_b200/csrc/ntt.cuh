@@ -31,16 +31,29 @@ constexpr int kTileWords = 4096;
 constexpr int kRowPad = 272;  // 256 words + one pad word per 16
 
 // A batch of tower transforms: slot y (blockIdx.y) of polynomial z
-// (blockIdx.z) lives at base + z * poly_stride + off[y] * N and uses the tables
-// of global tower id[y].
+// (blockIdx.z) is read at src + z * src_stride + off[y] * N, written at
+// dst + z * dst_stride + off[y] * N, and uses the tables of global tower id[y].
+// Optional destination split: with dst_odd set, polynomial z is written at
+// (z odd ? dst_odd : dst) + (z / 2) * dst_stride (the b and a channels of a
+// key switch land in separate caller buffers).
+// Optional forward epilogue (ModDown tail, include/ntt/resident_conversion.hpp:45-49):
+// with epi_left set, the last forward pass writes (left - ntt(x)) * pinv[id].
 constexpr int kMaxSlots = 128;
 struct NttBatch {
   u64 *dst;
   const u64 *src;
-  u64 poly_stride;
+  u64 src_stride, dst_stride;
+  u64 *dst_odd;
+  const u64 *epi_left;
+  u64 epi_left_stride;
+  const Shoup *epi_pinv;
   uint32_t off[kMaxSlots];
   uint16_t id[kMaxSlots];
 };
+
+#ifndef NTT_MINB
+#define NTT_MINB 4
+#endif
 
 struct TowerView {
   const TowerConsts *c;
@@ -53,12 +66,13 @@ __device__ __forceinline__ TowerView tower_view(const NttBatch &b, const DeviceT
   const uint32_t slot = blockIdx.y;
   const uint32_t g = b.id[slot];
   const u64 n = u64(1) << T.logn;
-  const u64 offset = blockIdx.z * b.poly_stride + u64(b.off[slot]) * n;
+  const u64 offset = u64(b.off[slot]) * n;
   TowerView v;
   v.c = T.tc + g;
   v.tw = (inv ? T.inv : T.fwd) + g * n;
-  v.src = b.src + offset;
-  v.dst = b.dst + offset;
+  const u64 z = blockIdx.z;
+  v.src = b.src + z * b.src_stride + offset;
+  v.dst = (b.dst_odd ? ((z & 1) ? b.dst_odd : b.dst) + (z >> 1) * b.dst_stride : b.dst + z * b.dst_stride) + offset;
   return v;
 }
 
@@ -110,7 +124,7 @@ struct ColGeom {
 };
 
 template <int LOGN, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) ntt_fwd_col(NttBatch b, DeviceTables T) {
+__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
   __shared__ u64 tile[kTileWords];
@@ -167,7 +181,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_fwd_col(NttBatch b, DeviceTab
 }
 
 template <int LOGN, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) ntt_inv_col(NttBatch b, DeviceTables T) {
+__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
   __shared__ u64 tile[kTileWords];
@@ -230,7 +244,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_inv_col(NttBatch b, DeviceTab
 __device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
 
 template <int LOGN, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) ntt_fwd_row(NttBatch b, DeviceTables T) {
+__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
   __shared__ u64 tile[16 * kRowPad];
   const TowerView v = tower_view(b, T, false);
@@ -278,11 +292,27 @@ __global__ void __launch_bounds__(kNttThreads) ntt_fwd_row(NttBatch b, DeviceTab
     my[pad_col(u * 16 + e)] = x[e];
   }
   __syncthreads();
-  store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+  if (b.epi_left == nullptr) {
+    store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+    return;
+  }
+  const u64 *left = b.epi_left + blockIdx.z * b.epi_left_stride + u64(b.off[blockIdx.y]) * (u64(1) << T.logn) +
+                    row0 * 256;
+  const Shoup pinv = b.epi_pinv[b.id[blockIdx.y]];
+  u64 *out = v.dst + row0 * 256;
+  for (int j = threadIdx.x; j < 16 * 128; j += kNttThreads) {
+    const int rr = j >> 7, c = (j & 127) * 2;
+    const int sidx = rr * kRowPad + pad_col(c);
+    const ulonglong2 l = *reinterpret_cast<const ulonglong2 *>(left + rr * 256 + c);
+    ulonglong2 o;
+    o.x = shoup_canon(sub_mod(l.x, tile[sidx], q), pinv.w, pinv.wq, q);
+    o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
+    *reinterpret_cast<ulonglong2 *>(out + rr * 256 + c) = o;
+  }
 }
 
 template <int LOGN, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) ntt_inv_row(NttBatch b, DeviceTables T) {
+__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
   __shared__ u64 tile[16 * kRowPad];
   const TowerView v = tower_view(b, T, true);

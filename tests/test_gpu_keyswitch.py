@@ -92,3 +92,47 @@ def test_bench_shape_keyswitch_full_size(lib, orc):
     wb, wa = orc.keyswitch(ctx, 24, x, kb, ka)
     np.testing.assert_array_equal(nb.to_host(ob), wb)
     np.testing.assert_array_equal(nb.to_host(oa), wa)
+
+
+@pytest.mark.parametrize("rotate", [False, True])
+def test_keyswitch_batch_equals_per_request(lib, orc, rotate):
+    """One batched launch sequence equals the oracle on every request."""
+    ctx = synthetic_context(orc, 8192, 6, 3, 2)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka = full_keys(orc, ctx, 17)
+    level, batch = 5, 5
+    xs = np.stack([orc.lcg(ctx.n, ctx.q[:level], 40 + r) for r in range(batch)])
+    c0 = np.stack([orc.lcg(ctx.n, ctx.q[:level], 80 + r) for r in range(batch)]) if rotate else None
+    ob, oa = nb.empty(xs.shape), nb.empty(xs.shape)
+    g.keyswitch_batch(level, batch, ob, oa, nb.to_device(xs), nb.to_device(kb), nb.to_device(ka),
+                      g.workspace(nb.OP_KEYSWITCH, level, batch),
+                      c0=None if c0 is None else nb.to_device(c0), automorphism=25 if rotate else 0)
+    got_b, got_a = nb.to_host(ob), nb.to_host(oa)
+    for r in range(batch):
+        wb, wa = orc.keyswitch(ctx, level, xs[r], kb, ka, None if c0 is None else c0[r], 25 if rotate else 0)
+        np.testing.assert_array_equal(got_b[r], wb)
+        np.testing.assert_array_equal(got_a[r], wa)
+
+
+def test_full_size_golden_digests(lib, orc):
+    """N = 65536 outputs equal the digests of the reference's own CPU path."""
+    import golden_cases as gc
+    d = gc.digests()
+    contexts = {}
+    for name, ctx, level, x, (kb, ka), c0, auto in gc.full_size_cases(orc):
+        key = (ctx.n, tuple(ctx.q), tuple(ctx.p))
+        if key not in contexts:
+            contexts[key] = (nb.Context.from_oracle(ctx), nb.to_device(kb), nb.to_device(ka))
+        g, dkb, dka = contexts[key]
+        ob, oa = nb.empty((level, ctx.n)), nb.empty((level, ctx.n))
+        g.keyswitch(level, ob, oa, nb.to_device(x), dkb, dka, g.workspace(nb.OP_KEYSWITCH, level),
+                    c0=None if c0 is None else nb.to_device(c0), automorphism=auto)
+        assert gc.sha(nb.to_host(ob)) == d[name + "_b"], name
+        assert gc.sha(nb.to_host(oa)) == d[name + "_a"], name
+    for name, q, psi, x in gc.ntt_cases(orc):
+        g = nb.Context(65536, [q], [psi])
+        out = nb.empty(x.shape)
+        g.ntt(out, nb.to_device(x), [0])
+        assert gc.sha(nb.to_host(out)) == d[f"ntt_{name}_forward"]
+        g.ntt(out, nb.to_device(x), [0], inverse=True)
+        assert gc.sha(nb.to_host(out)) == d[f"ntt_{name}_inverse"]
