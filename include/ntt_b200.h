@@ -40,6 +40,7 @@ extern "C" {
 #define NTT_B200_ERR_UNSUPPORTED 3 /* valid input outside this build's capability */
 #define NTT_B200_ERR_WORKSPACE 4   /* workspace missing or too small */
 #define NTT_B200_ERR_TIMEOUT 5     /* a bounded device wait expired */
+#define NTT_B200_NOT_READY 6       /* event query: recorded work has not completed yet */
 
 typedef struct ntt_b200_context_s *ntt_b200_context;
 
@@ -156,6 +157,35 @@ int ntt_b200_keyswitch_batch(ntt_b200_context ctx, size_t level, size_t batch, u
                              uint64_t *out_a, const uint64_t *src, const uint64_t *key_b,
                              const uint64_t *key_a, const uint64_t *c0, uint32_t automorphism,
                              void *workspace, size_t workspace_bytes, void *stream);
+
+/* MAC with per-digit device pointers (count digits of L+K towers each):
+ * full_key_rows != 0 -> key pointers are full-context digits (rows chosen by
+ * key_indices); 0 -> keys are already packed active QP rows. accumulate != 0
+ * adds into out_b/out_a instead of overwriting them. With count = 1 this is
+ * the reference's per-digit Driver::hybrid_mac (first_digit = !accumulate;
+ * src/cuda/resident_adapter.inc:31-43, 214-231). */
+int ntt_b200_hybrid_mac_digits(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                               const uint64_t *const *digits, const uint64_t *const *key_b,
+                               const uint64_t *const *key_a, size_t count, int full_key_rows,
+                               int accumulate, void *stream);
+
+/* Transport: streams, stream-ordered device memory, copies and events. These
+ * replace the reference CUDA Driver's Context stream, Buffer (one cudaMalloc
+ * per buffer) and Event plumbing (src/cuda/resident_adapter.inc:60-302).
+ * Device memory comes from the device's stream-ordered pool (kept cached).
+ * memcpy kind: 1 host->device, 2 device->host, 3 device->device (async). */
+int ntt_b200_stream_create(int device, void **stream);
+int ntt_b200_stream_destroy(void *stream);
+int ntt_b200_stream_synchronize(void *stream);
+int ntt_b200_alloc(int device, size_t bytes, void *stream, void **ptr);
+int ntt_b200_free(void *ptr, void *stream);
+int ntt_b200_memcpy(void *dst, const void *src, size_t bytes, int kind, void *stream);
+int ntt_b200_event_create(int device, void **event);
+int ntt_b200_event_destroy(void *event);
+int ntt_b200_event_record(void *event, void *stream);
+/* NTT_B200_OK when the recorded work completed, NTT_B200_NOT_READY otherwise. */
+int ntt_b200_event_query(void *event);
+int ntt_b200_event_synchronize(void *event);
 
 /* Opt-in per-kernel timing: while enabled, every launch of this library is
  * bracketed by CUDA events on its own stream. query() waits for the recorded

@@ -20,7 +20,7 @@ from .build import LIB
 __all__ = ["ContractError", "CudaError", "WorkspaceError", "Context", "library", "load",
            "kernel_launches", "OP_MOD_UP", "OP_MOD_DOWN", "OP_DIGITS", "OP_KEYSWITCH"]
 
-OK, ERR_CONTRACT, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_TIMEOUT = range(6)
+OK, ERR_CONTRACT, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_TIMEOUT, NOT_READY = range(7)
 OP_MOD_UP, OP_MOD_DOWN, OP_DIGITS, OP_KEYSWITCH = 1, 2, 3, 4
 
 
@@ -62,6 +62,18 @@ _SIGNATURES = {
     "ntt_b200_hybrid_digits": ([_P, _SZ, _P, _P, _P, _SZ, _P], _I),
     "ntt_b200_keyswitch": ([_P, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
     "ntt_b200_keyswitch_batch": ([_P, _SZ, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
+    "ntt_b200_hybrid_mac_digits": ([_P, _SZ, _P, _P, _P, _P, _P, _SZ, _I, _I, _P], _I),
+    "ntt_b200_stream_create": ([_I, ctypes.POINTER(_P)], _I),
+    "ntt_b200_stream_destroy": ([_P], _I),
+    "ntt_b200_stream_synchronize": ([_P], _I),
+    "ntt_b200_alloc": ([_I, _SZ, _P, ctypes.POINTER(_P)], _I),
+    "ntt_b200_free": ([_P, _P], _I),
+    "ntt_b200_memcpy": ([_P, _P, _SZ, _I, _P], _I),
+    "ntt_b200_event_create": ([_I, ctypes.POINTER(_P)], _I),
+    "ntt_b200_event_destroy": ([_P], _I),
+    "ntt_b200_event_record": ([_P, _P], _I),
+    "ntt_b200_event_query": ([_P], _I),
+    "ntt_b200_event_synchronize": ([_P], _I),
     "ntt_b200_timing_enable": ([_I], _I),
     "ntt_b200_timing_reset": ([], _I),
     "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),

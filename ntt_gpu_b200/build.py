@@ -14,6 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libntt_b200.so")
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(LIB_DIR, "libntt_b200_host.so")
+CXX_FLAGS = ["-std=c++20", "-O2", "-Wall", "-Wextra", "-fPIC", "-shared"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -23,25 +26,55 @@ def sources() -> list[str]:
                   if f.endswith((".cu", ".cuh", ".h", ".hpp")))
 
 
-def stale() -> bool:
-    if not os.path.exists(LIB):
+def host_sources() -> list[str]:
+    out = []
+    for sub in ("src", os.path.join("include", "ntt_b200")):
+        d = os.path.join(HOST, sub)
+        out += sorted(os.path.join(d, f) for f in os.listdir(d))
+    return out
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
         return True
-    built = os.path.getmtime(LIB)
-    deps = sources() + [os.path.join(HERE, "..", "include", "ntt_b200.h"), __file__]
+    built = os.path.getmtime(target)
     return any(os.path.getmtime(p) > built for p in deps if os.path.exists(p))
+
+
+def stale() -> bool:
+    header = os.path.join(HERE, "..", "include", "ntt_b200.h")
+    return (_stale(LIB, sources() + [header, __file__]) or
+            _stale(HOST_LIB, host_sources() + [header, __file__, LIB]))
+
+
+def build_host(verbose: bool = False) -> str:
+    """C++ resident runtime (Session + B200 driver) linked against libntt_b200.so."""
+    cxx = shutil.which("g++") or "g++"
+    tmp = HOST_LIB + ".tmp"
+    srcs = [os.path.join(HOST, "src", f) for f in ("session.cpp", "b200_driver.cpp")]
+    cmd = [cxx, *CXX_FLAGS, "-I", os.path.join(HOST, "include"), "-o", tmp, *srcs,
+           "-L", LIB_DIR, "-lntt_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, HOST_LIB)
+    return HOST_LIB
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
-    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    header = os.path.join(HERE, "..", "include", "ntt_b200.h")
     os.makedirs(LIB_DIR, exist_ok=True)
-    tmp = LIB + ".tmp"
-    cmd = [nvcc, *NVCC_FLAGS, "-o", tmp, os.path.join(CSRC, "capi.cu")]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
+    if force or _stale(LIB, sources() + [header, __file__]):
+        nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+        tmp = LIB + ".tmp"
+        cmd = [nvcc, *NVCC_FLAGS, "-o", tmp, os.path.join(CSRC, "capi.cu")]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB)
+    build_host(verbose)
     return LIB
 
 

@@ -89,29 +89,21 @@ __device__ __forceinline__ u64 reduce4(u64 x, u64 q, u64 q2) { return csub(csub(
 
 // ---- 128-bit accumulation ------------------------------------------------------
 // Exact sums of u64 products for the approximate-CRT basis switch and the Hybrid
-// MAC. A third word counts carries out of 128 bits (sums of up to 2^64 terms).
-struct Acc192 {
-  u64 lo, hi, top;
-};
-__device__ __forceinline__ void acc_zero(Acc192 &a) { a.lo = a.hi = a.top = 0; }
-__device__ __forceinline__ void acc_mad(Acc192 &a, u64 x, u64 y) {
-  const u64 plo = x * y, phi = mulhi(x, y);
-  asm("add.cc.u64 %0, %0, %3;\n\t"
-      "addc.cc.u64 %1, %1, %4;\n\t"
-      "addc.u64 %2, %2, 0;"
-      : "+l"(a.lo), "+l"(a.hi), "+l"(a.top)
-      : "l"(plo), "l"(phi));
-}
-// Without the carry word: the caller guarantees the sum stays below 2^128.
+// MAC, on the compiler's native 128-bit integers. Acc192 adds a word counting
+// carries out of 128 bits (for sums that may reach 2^128).
+using u128 = unsigned __int128;
 struct Acc128 {
-  u64 lo, hi;
+  u128 v = 0;
 };
-__device__ __forceinline__ void acc_mad(Acc128 &a, u64 x, u64 y) {
-  const u64 plo = x * y, phi = mulhi(x, y);
-  asm("add.cc.u64 %0, %0, %2;\n\t"
-      "addc.u64 %1, %1, %3;"
-      : "+l"(a.lo), "+l"(a.hi)
-      : "l"(plo), "l"(phi));
+__device__ __forceinline__ void acc_mad(Acc128 &a, u64 x, u64 y) { a.v += (u128)x * y; }
+struct Acc192 {
+  u128 v = 0;
+  u64 top = 0;
+};
+__device__ __forceinline__ void acc_mad(Acc192 &a, u64 x, u64 y) {
+  const u128 before = a.v;
+  a.v += (u128)x * y;
+  a.top += a.v < before;
 }
 
 // Reduction constants of a modulus m (m < 2^63):
@@ -126,19 +118,34 @@ struct Reducer {
 __device__ __forceinline__ u64 reduce64(u64 x, const Reducer &r) {
   return csub(x - mulhi(x, r.one) * r.m, r.m);
 }
-// (hi * 2^64 + lo) mod m.
+// v mod m in [0, 4m) (m < 2^62): hi * (2^64 mod m) and lo each reduced to [0, 2m).
+__device__ __forceinline__ u64 reduce128_lazy(u128 v, const Reducer &r) {
+  const u64 hi = (u64)(v >> 64), lo = (u64)v;
+  return shoup_lazy(hi, r.r64, r.r64q, r.m) + (lo - mulhi(lo, r.one) * r.m);
+}
+// (hi * 2^64 + lo) mod m, canonical, for any m < 2^63.
 __device__ __forceinline__ u64 reduce128(u64 lo, u64 hi, const Reducer &r) {
   const u64 a = csub(shoup_lazy(hi, r.r64, r.r64q, r.m), r.m);
   const u64 b = reduce64(lo, r);
   return add_mod(a, b, r.m);
 }
 __device__ __forceinline__ u64 reduce(const Acc128 &a, const Reducer &r) {
-  return reduce128(a.lo, a.hi, r);
+  return reduce128((u64)a.v, (u64)(a.v >> 64), r);
 }
 __device__ __forceinline__ u64 reduce(const Acc192 &a, const Reducer &r) {
-  const u64 low = reduce128(a.lo, a.hi, r);
+  const u64 low = reduce128((u64)a.v, (u64)(a.v >> 64), r);
   const u64 top = csub(shoup_lazy(a.top, r.r128, r.r128q, r.m), r.m);
   return add_mod(low, top, r.m);
+}
+// Result in [0, 4m) when the sum is below 2^128 and m < 2^62; canonical otherwise.
+template <bool LAZY>
+__device__ __forceinline__ u64 reduce_out(const Acc128 &a, const Reducer &r) {
+  if constexpr (LAZY) return reduce128_lazy(a.v, r);
+  else return reduce(a, r);
+}
+template <bool LAZY>
+__device__ __forceinline__ u64 reduce_out(const Acc192 &a, const Reducer &r) {
+  return reduce(a, r);
 }
 // a * b mod m for canonical a, b.
 __device__ __forceinline__ u64 mul_mod(u64 a, u64 b, const Reducer &r) {

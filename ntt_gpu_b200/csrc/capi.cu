@@ -440,15 +440,19 @@ std::vector<uint16_t> qp_ids(const Ctx &c, size_t level) {
 
 // ---- conversion launches ---------------------------------------------------------
 template <int MAXS>
-void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, cudaStream_t st) {
+void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, bool lazy_out, cudaStream_t st) {
   if (p.wide)
-    b200::conv_kernel<MAXS, true><<<grid, b200::kEwThreads, 0, st>>>(a);
+    b200::conv_kernel<MAXS, true, false><<<grid, b200::kEwThreads, 0, st>>>(a);
+  else if (lazy_out)
+    b200::conv_kernel<MAXS, false, true><<<grid, b200::kEwThreads, 0, st>>>(a);
   else
-    b200::conv_kernel<MAXS, false><<<grid, b200::kEwThreads, 0, st>>>(a);
+    b200::conv_kernel<MAXS, false, false><<<grid, b200::kEwThreads, 0, st>>>(a);
 }
+// lazy_out: outputs in [0, 4m), only for a lazy forward NTT that consumes them.
 void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
               const std::vector<uint16_t> &slots, size_t polys, u64 src_stride, u64 dst_stride,
-              cudaStream_t st) {
+              cudaStream_t st, bool lazy_out = false) {
+  lazy_out = lazy_out && c.lazy && c.logn >= 12;
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   b200::ConvArgs a{};
   a.plan = p.device;
@@ -469,10 +473,10 @@ void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
   const dim3 grid((unsigned)((c.n + b200::kEwThreads - 1) / b200::kEwThreads),
                   (unsigned)((p.t + a.targets_per_block - 1) / a.targets_per_block), (unsigned)polys);
   Timed t("conv", st);
-  if (p.s <= 4) launch_conv_t<4>(p, a, grid, st);
-  else if (p.s <= 8) launch_conv_t<8>(p, a, grid, st);
-  else if (p.s <= 16) launch_conv_t<16>(p, a, grid, st);
-  else launch_conv_t<40>(p, a, grid, st);
+  if (p.s <= 4) launch_conv_t<4>(p, a, grid, lazy_out, st);
+  else if (p.s <= 8) launch_conv_t<8>(p, a, grid, lazy_out, st);
+  else if (p.s <= 16) launch_conv_t<16>(p, a, grid, lazy_out, st);
+  else launch_conv_t<40>(p, a, grid, lazy_out, st);
   t.done();
 }
 
@@ -523,7 +527,7 @@ void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst
   const auto &plan = c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L));
   std::vector<uint16_t> slots;
   for (size_t i = 0; i < L; ++i) slots.push_back((uint16_t)i);
-  run_conv(c, plan, corr, p_coeff, slots, polys, K * n, L * n, st);
+  run_conv(c, plan, corr, p_coeff, slots, polys, K * n, L * n, st, true);
   NttFinal fin;
   fin.dst = dst;
   fin.dst_odd = dst_odd;
@@ -562,34 +566,41 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
         fwd.push_back({(uint32_t)(digit * T + t), all[t]});
       }
     const auto &plan = c.conv_plan(range_ids(first, first + count), tgt);
-    run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st);
+    run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st, true);
   }
   run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st);
 }
 
-// MAC of `polys` requests: out_b/out_a of request z at out + z * out_stride.
-void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride, const u64 *digits,
-            const u64 *input, const u64 *key_b, const u64 *key_a, cudaStream_t st) {
+// MAC of `polys` requests: out_b/out_a of request z at out + z * out_stride;
+// digit d of request z at digits[d] + z * digit_poly_stride.
+void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride,
+            const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
+            const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a, bool full_key_rows,
+            bool accumulate, cudaStream_t st) {
   const size_t n = c.n, T = L + c.k;
-  const size_t beta = 1 + (L - 1) / c.alpha;
+  const size_t beta = digits.size();
+  require(beta >= 1 && beta <= (size_t)b200::kMaxDigits && key_b.size() == beta && key_a.size() == beta,
+          "MAC digit count out of range");
   b200::MacArgs a{};
   a.out_b = out_b;
   a.out_a = out_a;
-  a.digits = digits;
+  for (size_t d = 0; d < beta; ++d) {
+    a.digit[d] = digits[d];
+    a.key_b[d] = key_b[d];
+    a.key_a[d] = key_a[d];
+  }
   a.input = input;
-  a.key_b = key_b;
-  a.key_a = key_a;
   a.tc = c.d_tc;
-  a.digit_stride = T * n;
-  a.key_digit_stride = c.towers() * n;
   a.poly_stride_out = out_stride;
-  a.poly_stride_digits = beta * T * n;
+  a.poly_stride_digits = digit_poly_stride;
   a.poly_stride_input = L * n;
   a.level = (int)L;
   a.m = (int)c.m;
   a.beta = (int)beta;
   a.alpha = (int)c.alpha;
   a.logn = c.logn;
+  a.full_key_rows = full_key_rows;
+  a.accumulate = accumulate;
   u64 max_q = 0;
   for (auto q : c.mod) max_q = std::max(max_q, q);
   const u128 prod = (u128)(max_q - 1) * (max_q - 1);
@@ -601,6 +612,13 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
   else
     b200::mac_kernel<false><<<grid, b200::kEwThreads, 0, st>>>(a);
   t.done();
+}
+
+// Full-context key digits d at key + d * (M + K) * N.
+std::vector<const u64 *> key_digits(const Ctx &c, const u64 *key, size_t beta) {
+  std::vector<const u64 *> v;
+  for (size_t d = 0; d < beta; ++d) v.push_back(key + d * c.towers() * c.n);
+  return v;
 }
 
 void do_rotate(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,
@@ -635,7 +653,10 @@ void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const 
   u64 *acc = ws.take(2 * batch * T * n);  // [batch][b|a][T][N]
   u64 *rot = ws.take(2 * batch * T * n);
   do_digits(c, L, batch, digits, src, ws, false, st);
-  do_mac(c, L, batch, acc, acc + T * n, 2 * T * n, digits, src, key_b, key_a, st);
+  std::vector<const u64 *> dptr;
+  for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
+  do_mac(c, L, batch, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, src, key_digits(c, key_b, beta),
+         key_digits(c, key_a, beta), true, false, st);
   const u64 *ext = acc;
   if (c0) {
     do_rotate(c, L, batch, rot, rot + T * n, acc, acc + T * n, 2 * T * n, c0, L * n, g, st);
@@ -898,7 +919,11 @@ int ntt_b200_hybrid_mac(ntt_b200_context ctx, size_t level, uint64_t *out_b, uin
     require(out_b && out_a && digits && key_b && key_a, "null pointer");
     require_aligned({out_b, out_a, digits, key_b, key_a});
     DeviceGuard guard(ctx->device);
-    do_mac(*ctx, level, 1, out_b, out_a, 0, digits, nullptr, key_b, key_a, as_stream(stream));
+    const size_t beta = 1 + (level - 1) / ctx->alpha, T = level + ctx->k;
+    std::vector<const u64 *> dptr;
+    for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * ctx->n);
+    do_mac(*ctx, level, 1, out_b, out_a, 0, dptr, 0, nullptr, key_digits(*ctx, key_b, beta),
+           key_digits(*ctx, key_a, beta), true, false, as_stream(stream));
   });
 }
 
@@ -948,7 +973,7 @@ int ntt_b200_mod_up(ntt_b200_context ctx, size_t level, uint64_t *dst, const uin
     const auto &plan = c.conv_plan(range_ids(0, L), range_ids(c.m, c.m + K));
     std::vector<uint16_t> slots;
     for (size_t i = 0; i < K; ++i) slots.push_back((uint16_t)(L + i));
-    run_conv(c, plan, dst, coeff, slots, 1, 0, 0, st);
+    run_conv(c, plan, dst, coeff, slots, 1, 0, 0, st, true);
     run_ntt(c, dst, dst, contiguous_slots(range_ids(c.m, c.m + K), (uint32_t)L), 1, 0, 0, false, st);
   });
 }
@@ -1002,6 +1027,126 @@ int ntt_b200_keyswitch_batch(ntt_b200_context ctx, size_t level, size_t batch, u
     Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_KEYSWITCH, level, batch);
     DeviceGuard guard(c.device);
     do_keyswitch(c, level, batch, out_b, out_a, src, key_b, key_a, c0, automorphism, ws, as_stream(stream));
+  });
+}
+
+int ntt_b200_hybrid_mac_digits(ntt_b200_context ctx, size_t level, uint64_t *out_b, uint64_t *out_a,
+                               const uint64_t *const *digits, const uint64_t *const *key_b,
+                               const uint64_t *const *key_a, size_t count, int full_key_rows, int accumulate,
+                               void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(out_b && out_a && digits && key_b && key_a, "null pointer");
+    require(count >= 1 && count <= (size_t)b200::kMaxDigits, "MAC digit count out of range");
+    std::vector<const u64 *> d, kb, ka;
+    for (size_t i = 0; i < count; ++i) {
+      require(digits[i] && key_b[i] && key_a[i], "null digit or key pointer");
+      require_aligned({digits[i], key_b[i], key_a[i]});
+      d.push_back(digits[i]);
+      kb.push_back(key_b[i]);
+      ka.push_back(key_a[i]);
+    }
+    require_aligned({out_b, out_a});
+    DeviceGuard guard(ctx->device);
+    do_mac(*ctx, level, 1, out_b, out_a, 0, d, 0, nullptr, kb, ka, full_key_rows != 0, accumulate != 0,
+           as_stream(stream));
+  });
+}
+
+// ---- transport -----------------------------------------------------------------------
+int ntt_b200_stream_create(int device, void **stream) {
+  return guarded([&] {
+    require(stream != nullptr && device >= 0, "invalid stream request");
+    DeviceGuard guard(device);
+    cudaMemPool_t pool;
+    CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool
+    CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    cudaStream_t s = nullptr;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *stream = s;
+  });
+}
+
+int ntt_b200_stream_destroy(void *stream) {
+  return guarded([&] {
+    if (stream) CUDA_CHECK(cudaStreamDestroy(as_stream(stream)));
+  });
+}
+
+int ntt_b200_stream_synchronize(void *stream) {
+  return guarded([&] { CUDA_CHECK(cudaStreamSynchronize(as_stream(stream))); });
+}
+
+int ntt_b200_alloc(int device, size_t bytes, void *stream, void **ptr) {
+  return guarded([&] {
+    require(ptr != nullptr && device >= 0, "invalid allocation request");
+    *ptr = nullptr;
+    DeviceGuard guard(device);
+    CUDA_CHECK(cudaMallocAsync(ptr, std::max<size_t>(bytes, 256), as_stream(stream)));
+  });
+}
+
+int ntt_b200_free(void *ptr, void *stream) {
+  return guarded([&] {
+    if (ptr) CUDA_CHECK(cudaFreeAsync(ptr, as_stream(stream)));
+  });
+}
+
+int ntt_b200_memcpy(void *dst, const void *src, size_t bytes, int kind, void *stream) {
+  return guarded([&] {
+    require(dst && src, "null pointer");
+    require(kind >= 1 && kind <= 3, "copy kind must be 1 (to device), 2 (to host) or 3 (device to device)");
+    const cudaMemcpyKind k = kind == 1 ? cudaMemcpyHostToDevice
+                             : kind == 2 ? cudaMemcpyDeviceToHost
+                                         : cudaMemcpyDeviceToDevice;
+    if (bytes) CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, k, as_stream(stream)));
+  });
+}
+
+int ntt_b200_event_create(int device, void **event) {
+  return guarded([&] {
+    require(event != nullptr && device >= 0, "invalid event request");
+    DeviceGuard guard(device);
+    cudaEvent_t e = nullptr;
+    CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    *event = e;
+  });
+}
+
+int ntt_b200_event_destroy(void *event) {
+  return guarded([&] {
+    if (event) CUDA_CHECK(cudaEventDestroy(reinterpret_cast<cudaEvent_t>(event)));
+  });
+}
+
+int ntt_b200_event_record(void *event, void *stream) {
+  return guarded([&] {
+    require(event != nullptr, "null event");
+    CUDA_CHECK(cudaEventRecord(reinterpret_cast<cudaEvent_t>(event), as_stream(stream)));
+  });
+}
+
+int ntt_b200_event_query(void *event) {
+  if (!event) {
+    g_last_error = "null event";
+    return NTT_B200_ERR_CONTRACT;
+  }
+  const cudaError_t e = cudaEventQuery(reinterpret_cast<cudaEvent_t>(event));
+  if (e == cudaSuccess) return NTT_B200_OK;
+  if (e == cudaErrorNotReady) {
+    (void)cudaGetLastError();
+    return NTT_B200_NOT_READY;
+  }
+  g_last_error = std::string("CUDA: cudaEventQuery: ") + cudaGetErrorString(e);
+  return NTT_B200_ERR_CUDA;
+}
+
+int ntt_b200_event_synchronize(void *event) {
+  return guarded([&] {
+    require(event != nullptr, "null event");
+    CUDA_CHECK(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(event)));
   });
 }
 

@@ -26,7 +26,9 @@ struct ConvArgs {
   int targets_per_block;
 };
 
-template <int MAXS, bool WIDE>
+// LAZY_OUT: outputs in [0, 4m) for a lazy forward NTT that consumes them
+// directly (it accepts [0, 4q) inputs); otherwise canonical.
+template <int MAXS, bool WIDE, bool LAZY_OUT>
 __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
   __shared__ u64 hat[MAXS * kMaxConvTargets];
   __shared__ Reducer red[kMaxConvTargets];
@@ -56,23 +58,25 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
 #pragma unroll
   for (int j = 0; j < MAXS; ++j)
     if (j < s) y[j] = shoup_canon(src[j * n + k], sinv[j].w, sinv[j].wq, sq[j]);
-  for (int t = 0; t < nt; ++t) {
-    u64 out;
-    if constexpr (WIDE) {
-      Acc192 acc;
-      acc_zero(acc);
+  using Acc = typename std::conditional<WIDE, Acc192, Acc128>::type;
+  int t = 0;
+  for (; t + 1 < nt; t += 2) {
+    Acc a0{}, a1{};
 #pragma unroll
-      for (int j = 0; j < MAXS; ++j)
-        if (j < s) acc_mad(acc, y[j], hat[j * nt + t]);
-      out = reduce(acc, red[t]);
-    } else {
-      Acc128 acc{0, 0};
+    for (int j = 0; j < MAXS; ++j)
+      if (j < s) {
+        acc_mad(a0, y[j], hat[j * nt + t]);
+        acc_mad(a1, y[j], hat[j * nt + t + 1]);
+      }
+    dst[u64(a.slot[t0 + t]) * n + k] = reduce_out<LAZY_OUT>(a0, red[t]);
+    dst[u64(a.slot[t0 + t + 1]) * n + k] = reduce_out<LAZY_OUT>(a1, red[t + 1]);
+  }
+  if (t < nt) {
+    Acc a0{};
 #pragma unroll
-      for (int j = 0; j < MAXS; ++j)
-        if (j < s) acc_mad(acc, y[j], hat[j * nt + t]);
-      out = reduce(acc, red[t]);
-    }
-    dst[u64(a.slot[t0 + t]) * n + k] = out;
+    for (int j = 0; j < MAXS; ++j)
+      if (j < s) acc_mad(a0, y[j], hat[j * nt + t]);
+    dst[u64(a.slot[t0 + t]) * n + k] = reduce_out<LAZY_OUT>(a0, red[t]);
   }
 }
 
@@ -102,18 +106,21 @@ __global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
 
 // ---- Hybrid MAC over all digits in one pass --------------------------------------
 // Z_b[t] = sum_d D_d[t] * KB_d[row(t)], Z_a likewise (resident.cpp:530-570 with
-// hybrid_mac_value, resident_conversion.hpp:50-54). Keys are full-context:
-// digit d, row r at key + d * key_digit_stride + r * n; row(t) = t for active Q,
-// M + (t - L) for P (key_indices, backend_contract.hpp:112-119).
+// hybrid_mac_value, resident_conversion.hpp:50-54). Keys are either full-context
+// rows (row(t) = t for active Q, M + (t - L) for P: key_indices,
+// backend_contract.hpp:112-119) or already packed active rows (row(t) = t).
+// With accumulate set, the result is added to the existing outputs (the
+// reference's per-digit primitive for digits after the first).
+constexpr int kMaxDigits = 40;
 struct MacArgs {
   u64 *out_b, *out_a;
-  const u64 *digits;    // digit d, tower t at digits + d * digit_stride + t * n
-  const u64 *input;     // if set: digit d's own Q towers are read from input + t * n
-  const u64 *key_b, *key_a;
+  const u64 *digit[kMaxDigits];  // digit d, tower t at digit[d] + z * poly_stride_digits + t * n
+  const u64 *key_b[kMaxDigits], *key_a[kMaxDigits];
+  const u64 *input;              // if set: digit d's own Q towers are read from input + t * n
   const TowerConsts *tc;
-  u64 digit_stride, key_digit_stride;
   u64 poly_stride_out, poly_stride_digits, poly_stride_input;
   int level, m, beta, alpha, logn;
+  bool full_key_rows, accumulate;
 };
 // Grid: x = coefficient block, y = request, z = QP tower. Requests vary faster
 // than towers, so the key rows of one tower stay in L2 while every request of
@@ -127,20 +134,25 @@ __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
   if (i >= n) return;
   const int g = t < a.level ? t : a.m + (t - a.level);
   const Reducer red = a.tc[g].red;
-  const u64 *d = a.digits + z * a.poly_stride_digits + t * n + i;
+  const u64 row = a.full_key_rows ? u64(g) : u64(t);
   const int own = (a.input && t < a.level) ? t / a.alpha : -1;
-  const u64 *kb = a.key_b + u64(g) * n + i;
-  const u64 *ka = a.key_a + u64(g) * n + i;
+  const u64 doff = z * a.poly_stride_digits + t * n + i;
   using Acc = typename std::conditional<WIDE, Acc192, Acc128>::type;
   Acc ab{}, aa{};
+#pragma unroll 4
   for (int j = 0; j < a.beta; ++j) {
-    const u64 x = j == own ? a.input[z * a.poly_stride_input + t * n + i] : d[j * a.digit_stride];
-    acc_mad(ab, x, kb[j * a.key_digit_stride]);
-    acc_mad(aa, x, ka[j * a.key_digit_stride]);
+    const u64 x = j == own ? a.input[z * a.poly_stride_input + t * n + i] : a.digit[j][doff];
+    acc_mad(ab, x, a.key_b[j][row * n + i]);
+    acc_mad(aa, x, a.key_a[j][row * n + i]);
   }
   const u64 o = z * a.poly_stride_out + t * n + i;
-  a.out_b[o] = reduce(ab, red);
-  a.out_a[o] = reduce(aa, red);
+  u64 rb = reduce(ab, red), ra = reduce(aa, red);
+  if (a.accumulate) {
+    rb = add_mod(rb, a.out_b[o], red.m);
+    ra = add_mod(ra, a.out_a[o], red.m);
+  }
+  a.out_b[o] = rb;
+  a.out_a[o] = ra;
 }
 
 // ---- rotation: automorphism gather plus P*c0 on Q towers ------------------------
