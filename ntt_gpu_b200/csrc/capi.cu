@@ -8,18 +8,21 @@
 #include <cstdint>
 #include <initializer_list>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/ntt_b200.h"
 #include "arith.cuh"
 #include "kernels.cuh"
 #include "ntt.cuh"
+#include "ntt_ps.cuh"
 #include "tables.cuh"
 
 using b200::u64;
@@ -316,6 +319,50 @@ struct NttFinal {
   const b200::Shoup *epi_pinv = nullptr;
 };
 
+// Persistent double-buffered passes (ntt_ps.cuh): grid = resident CTAs of the
+// device; per-device launch attributes are set once.
+int device_sms(int device) {
+  static int sms[64] = {0};
+  if (device < 0 || device >= 64) throw ContractError("device ordinal out of range");
+  if (!sms[device]) CUDA_CHECK(cudaDeviceGetAttribute(&sms[device], cudaDevAttrMultiProcessorCount, device));
+  return sms[device];
+}
+template <class Kernel>
+unsigned persistent_grid(Kernel kernel, int smem, uint32_t total, int device, int *cache) {
+  if (!cache[device]) {
+    CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, b200::kNttThreads, smem));
+    cache[device] = std::max(1, per_sm);
+  }
+  const uint64_t resident = uint64_t(cache[device]) * device_sms(device);
+  return (unsigned)std::min<uint64_t>(total, resident);
+}
+bool persistent_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("NTT_B200_PERSISTENT");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+template <int LOGN, bool LAZY, bool INV>
+void launch_col_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
+  static int cache[64] = {0};
+  constexpr int smem = b200::col_smem_bytes<LOGN>();
+  const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
+  const unsigned grid = persistent_grid(b200::ntt_col_ps<LOGN, LAZY, INV>, smem, total, c.device, cache);
+  b200::ntt_col_ps<LOGN, LAZY, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
+}
+template <int LOGN, bool LAZY, bool INV>
+void launch_row_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
+  static int cache[64] = {0};
+  constexpr int smem = b200::kRowPsSmem;
+  const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
+  const unsigned grid = persistent_grid(b200::ntt_row_ps<LOGN, LAZY, INV>, smem, total, c.device, cache);
+  b200::ntt_row_ps<LOGN, LAZY, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
+}
+
 template <int LOGN, bool LAZY>
 void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
                       bool inverse, cudaStream_t st) {
@@ -330,6 +377,25 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     second.epi_left = fin->epi_left;
     second.epi_left_stride = fin->epi_left_stride;
     second.epi_pinv = fin->epi_pinv;
+  }
+  if (persistent_enabled()) {
+    const uint32_t ns = (uint32_t)slots, np = (uint32_t)polys;
+    if (!inverse) {
+      Timed t1("ntt_fwd_col", st);
+      launch_col_ps<LOGN, LAZY, false>(c, b, ns, np, st);
+      t1.done();
+      Timed t2("ntt_fwd_row", st);
+      launch_row_ps<LOGN, LAZY, false>(c, second, ns, np, st);
+      t2.done();
+    } else {
+      Timed t1("ntt_inv_row", st);
+      launch_row_ps<LOGN, LAZY, true>(c, b, ns, np, st);
+      t1.done();
+      Timed t2("ntt_inv_col", st);
+      launch_col_ps<LOGN, LAZY, true>(c, second, ns, np, st);
+      t2.done();
+    }
+    return;
   }
   if (!inverse) {
     Timed t1("ntt_fwd_col", st);
@@ -605,12 +671,29 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
   for (auto q : c.mod) max_q = std::max(max_q, q);
   const u128 prod = (u128)(max_q - 1) * (max_q - 1);
   const bool wide = prod > (~(u128)0) / (u128)beta;
-  const dim3 grid((unsigned)((n + b200::kEwThreads - 1) / b200::kEwThreads), (unsigned)polys, (unsigned)T);
   Timed t("mac", st);
-  if (wide)
-    b200::mac_kernel<true><<<grid, b200::kEwThreads, 0, st>>>(a);
-  else
-    b200::mac_kernel<false><<<grid, b200::kEwThreads, 0, st>>>(a);
+  if (n >= 2 * b200::kEwThreads && beta <= 4) {
+    const dim3 grid2((unsigned)(n / (2 * b200::kEwThreads)), (unsigned)polys, (unsigned)T);
+    auto launch = [&](auto beta_tag) {
+      constexpr int B = decltype(beta_tag)::value;
+      if (wide)
+        b200::mac2_kernel<B, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
+      else
+        b200::mac2_kernel<B, false><<<grid2, b200::kEwThreads, 0, st>>>(a);
+    };
+    switch (beta) {
+      case 1: launch(std::integral_constant<int, 1>{}); break;
+      case 2: launch(std::integral_constant<int, 2>{}); break;
+      case 3: launch(std::integral_constant<int, 3>{}); break;
+      default: launch(std::integral_constant<int, 4>{}); break;
+    }
+  } else {
+    const dim3 grid((unsigned)((n + b200::kEwThreads - 1) / b200::kEwThreads), (unsigned)polys, (unsigned)T);
+    if (wide)
+      b200::mac_kernel<true><<<grid, b200::kEwThreads, 0, st>>>(a);
+    else
+      b200::mac_kernel<false><<<grid, b200::kEwThreads, 0, st>>>(a);
+  }
   t.done();
 }
 

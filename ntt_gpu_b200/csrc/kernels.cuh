@@ -155,6 +155,51 @@ __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
   a.out_a[o] = ra;
 }
 
+// Same MAC with a compile-time digit count and two adjacent coefficients per
+// thread (16-byte loads of every digit and key row).
+template <int BETA, bool WIDE>
+__global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
+  const u64 n = u64(1) << a.logn;
+  const u64 i = (u64(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
+  const int t = blockIdx.z;
+  const u64 z = blockIdx.y;
+  if (i >= n) return;
+  const int g = t < a.level ? t : a.m + (t - a.level);
+  const Reducer red = a.tc[g].red;
+  const u64 row = a.full_key_rows ? u64(g) : u64(t);
+  const int own = (a.input && t < a.level) ? t / a.alpha : -1;
+  const u64 doff = z * a.poly_stride_digits + t * n + i;
+  using Acc = typename std::conditional<WIDE, Acc192, Acc128>::type;
+  Acc b0{}, b1{}, a0{}, a1{};
+#pragma unroll
+  for (int j = 0; j < BETA; ++j) {
+    const ulonglong2 x = j == own ? *reinterpret_cast<const ulonglong2 *>(a.input + z * a.poly_stride_input + t * n + i)
+                                  : *reinterpret_cast<const ulonglong2 *>(a.digit[j] + doff);
+    const ulonglong2 kb = *reinterpret_cast<const ulonglong2 *>(a.key_b[j] + row * n + i);
+    const ulonglong2 ka = *reinterpret_cast<const ulonglong2 *>(a.key_a[j] + row * n + i);
+    acc_mad(b0, x.x, kb.x);
+    acc_mad(b1, x.y, kb.y);
+    acc_mad(a0, x.x, ka.x);
+    acc_mad(a1, x.y, ka.y);
+  }
+  const u64 o = z * a.poly_stride_out + t * n + i;
+  ulonglong2 rb, ra;
+  rb.x = reduce(b0, red);
+  rb.y = reduce(b1, red);
+  ra.x = reduce(a0, red);
+  ra.y = reduce(a1, red);
+  if (a.accumulate) {
+    const ulonglong2 ob = *reinterpret_cast<const ulonglong2 *>(a.out_b + o);
+    const ulonglong2 oa = *reinterpret_cast<const ulonglong2 *>(a.out_a + o);
+    rb.x = add_mod(rb.x, ob.x, red.m);
+    rb.y = add_mod(rb.y, ob.y, red.m);
+    ra.x = add_mod(ra.x, oa.x, red.m);
+    ra.y = add_mod(ra.y, oa.y, red.m);
+  }
+  *reinterpret_cast<ulonglong2 *>(a.out_b + o) = rb;
+  *reinterpret_cast<ulonglong2 *>(a.out_a + o) = ra;
+}
+
 // ---- rotation: automorphism gather plus P*c0 on Q towers ------------------------
 // resident_adapter.inc:44-59 semantics with automorphism_source_index and
 // rotated_b_value (resident_conversion.hpp:15-29).
