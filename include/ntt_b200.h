@@ -187,6 +187,27 @@ int ntt_b200_event_record(void *event, void *stream);
 int ntt_b200_event_query(void *event);
 int ntt_b200_event_synchronize(void *event);
 
+/* Allocation-free ModDown. For callers that must not allocate device memory:
+ * hosts whose HBM is already owned by another caching allocator (a framework
+ * process that has reserved the device), latency-critical request threads that
+ * cannot afford cudaMalloc's implicit device synchronisation, and FFI hosts
+ * that have no way to own or release device buffers across the boundary.
+ * Same result as ntt_b200_mod_down, but the scratch is a file-scope device
+ * array of ntt_b200_mod_down_static_max_bytes() (8 MiB), which every GPU that
+ * loads this library holds until exit; (K + L) * N * 8 bytes must fit in it,
+ * larger requests are refused with a contract error. The caller still passes
+ * the input and output. The level's tables must exist already
+ * (ntt_b200_context_prepare); this call allocates nothing. Its first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture. All calls share the one array and
+ * it keeps the previous call's contents (nothing in it needs to start at zero):
+ * calls that overlap on the GPU - on different streams, or on one device from
+ * different contexts - race on it. This entry point has no counterpart in the
+ * reference. */
+size_t ntt_b200_mod_down_static_max_bytes(void);
+int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
+                             void *stream);
+
 /* Opt-in per-kernel timing: while enabled, every launch of this library is
  * bracketed by CUDA events on its own stream. query() waits for the recorded
  * events and returns the launch count and summed device time of one kernel

@@ -74,6 +74,8 @@ _SIGNATURES = {
     "ntt_b200_event_record": ([_P, _P], _I),
     "ntt_b200_event_query": ([_P], _I),
     "ntt_b200_event_synchronize": ([_P], _I),
+    "ntt_b200_mod_down_static_max_bytes": ([], _SZ),
+    "ntt_b200_mod_down_static": ([_P, _SZ, _P, _P, _P], _I),
     "ntt_b200_timing_enable": ([_I], _I),
     "ntt_b200_timing_reset": ([], _I),
     "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),

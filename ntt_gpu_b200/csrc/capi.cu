@@ -220,6 +220,18 @@ struct ntt_b200_context_s {
     return conv.emplace(key, hp).first->second;
   }
 
+  // Lookups that never build or upload a plan (nullptr when absent).
+  const HostConvPlan *find_conv_plan(const std::vector<uint16_t> &src, const std::vector<uint16_t> &tgt) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = conv.find(std::make_pair(src, tgt));
+    return it == conv.end() ? nullptr : &it->second;
+  }
+  b200::DownPlan *find_down_plan(size_t level) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = down.find(level);
+    return it == down.end() ? nullptr : it->second;
+  }
+
   b200::DownPlan *down_plan(size_t level) {
     std::lock_guard<std::mutex> lock(mu);
     auto it = down.find(level);
@@ -1233,4 +1245,54 @@ int ntt_b200_event_synchronize(void *event) {
   });
 }
 
+}  // extern "C"
+
+// ---- allocation-free ModDown ------------------------------------------------------------
+// Scratch of ntt_b200_mod_down_static: a file-scope device array every GPU that
+// loads this library holds until process exit. Host code never uses the
+// symbol's host-side name as a device address: the address comes from
+// cudaGetSymbolAddress, once per device, with that device current.
+constexpr size_t kStaticScratchWords = size_t(1) << 20;  // 8 MiB
+static __device__ __align__(256) uint64_t g_static_scratch[kStaticScratchWords];
+
+namespace {
+std::mutex g_static_mu;
+uint64_t *g_static_ptr[64] = {nullptr};
+
+uint64_t *static_scratch(int device) {
+  require(device >= 0 && device < 64, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[device]) {
+    DeviceGuard guard(device);
+    void *ptr = nullptr;
+    CUDA_CHECK(cudaGetSymbolAddress(&ptr, g_static_scratch));
+    g_static_ptr[device] = static_cast<uint64_t *>(ptr);
+  }
+  return g_static_ptr[device];
+}
+}  // namespace
+
+extern "C" {
+size_t ntt_b200_mod_down_static_max_bytes(void) { return kStaticScratchWords * sizeof(uint64_t); }
+
+int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
+                             void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(dst && src, "null pointer");
+    require_aligned({dst, src});
+    Ctx &c = *ctx;
+    const size_t need = workspace_bytes(c, NTT_B200_OP_MOD_DOWN, level, 1);
+    if (need > kStaticScratchWords * sizeof(uint64_t))
+      throw ContractError("ModDown scratch exceeds the 8 MiB static maximum of ntt_b200_mod_down_static "
+                          "(needs (K + L) * N * 8 bytes); use ntt_b200_mod_down with a workspace");
+    require(c.find_conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level)) && c.find_down_plan(level),
+            "ntt_b200_mod_down_static needs the level's tables: call ntt_b200_context_prepare(level) first");
+    uint64_t *scratch = static_scratch(c.device);
+    DeviceGuard guard(c.device);
+    Carver ws{reinterpret_cast<char *>(scratch), kStaticScratchWords * sizeof(uint64_t)};
+    do_mod_down(c, level, 1, dst, nullptr, 0, src, 0, ws, as_stream(stream));
+  });
+}
 }  // extern "C"
