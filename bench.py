@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-vs-plain Poisson legs")
     ap.add_argument("--kernels-only", action="store_true",
                     help="timed batched steps only (no plain/e2e/CPU legs); for profiler launch lists")
     return ap.parse_args()
@@ -230,6 +231,149 @@ def run_reference(args, rank, world):
 
 
 # ---- GPU side ------------------------------------------------------------------------------------
+# ---- serving: seeded Poisson arrivals through the continuous-batching server ---------------------
+def device_residues(n, moduli, seed, polys, device):
+    """[polys][towers][n] int64 tensor of residues in [0, q_t) from a seeded device generator."""
+    import torch
+    gen = torch.Generator(device=f"cuda:{device}")
+    gen.manual_seed(seed)
+    v = torch.randint(0, 1 << 62, (polys, len(moduli), n), generator=gen, dtype=torch.int64,
+                      device=f"cuda:{device}")
+    q = torch.tensor([int(m) for m in moduli], dtype=torch.int64, device=f"cuda:{device}")
+    return v % q[None, :, None]
+
+
+class Workload:
+    """Device-resident inputs, keys and an output ring of one context for served requests."""
+
+    def __init__(self, nb, prm, device, seed, n_inputs=4, n_keys=2, ring=48):
+        import torch
+        self.prm, self.device = prm, device
+        self.ctx = nb.Context(prm.n, prm.q, prm.q_psi, prm.p, prm.p_psi, prm.alpha, device)
+        for level in range(1, prm.m + 1):
+            self.ctx.prepare(level)
+        qp = prm.q + prm.p
+        self.inputs = device_residues(prm.n, prm.q, seed, n_inputs, device)
+        self.c0 = device_residues(prm.n, prm.q, seed + 1, n_inputs, device)
+        self.keys = [(device_residues(prm.n, qp, seed + 10 + 2 * i, prm.full_digits(), device),
+                      device_residues(prm.n, qp, seed + 11 + 2 * i, prm.full_digits(), device))
+                     for i in range(n_keys)]
+        self.out = torch.empty((ring, 2, prm.m, prm.n), dtype=torch.int64, device=f"cuda:{device}")
+        self.slot = 0
+
+    def request(self, nb, level, kind, step, i):
+        n = self.prm.n
+        out = self.out[self.slot % self.out.shape[0]]
+        self.slot += 1
+        x = self.inputs[i % self.inputs.shape[0]]
+        kb, ka = self.keys[i % len(self.keys)]
+        ob, oa = out[0, :level], out[1, :level]
+        if kind == "rotate":
+            g = pow(5, step % (n // 2), 2 * n)
+            return nb.make_request(level, x[:level], ob, oa, kb, ka, c0=self.c0[i % self.c0.shape[0]][:level],
+                                   automorphism=g)
+        if kind == "relin":
+            return nb.make_request(level, x[:level], ob, oa, kb, ka, add_b=ob, add_a=oa)
+        return nb.make_request(level, x[:level], ob, oa, kb, ka)
+
+
+def serve_poisson(nb, srv, jobs, rate, seed):
+    """Submit jobs [(ctx, request)] at seeded Poisson arrival times of `rate` per second, wait for all."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, len(jobs))
+    srv.stats(reset=True)
+    tickets = []
+    t_next = time.perf_counter()
+    for (ctx, req), gap in zip(jobs, gaps):
+        t_next += gap
+        while True:
+            now = time.perf_counter()
+            if now >= t_next:
+                break
+            if t_next - now > 3e-4:
+                time.sleep(t_next - now - 2e-4)
+        tickets.append(srv.submit(ctx, req))
+    waves = [srv.wait(t).wave_size for t in tickets]
+    st = srv.stats(reset=True)
+    return {"offered_per_s": rate, "throughput": st["throughput"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "max_ms": st["max_ms"], "mean_wave": sum(waves) / len(waves), "requests": len(jobs)}
+
+
+def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
+    """Served (continuous batching) vs plain (same kernels, one request per wave, one lane)."""
+    import numpy as np
+
+    from ntt_gpu_b200.params import synthetic_params
+    budget = 40 << 30
+    out = {"served_server": {"lanes": 2, "max_batch": BATCH, "hbm_budget_bytes": budget},
+           "plain_server": {"lanes": 1, "max_batch": 1, "hbm_budget_bytes": budget},
+           "arrivals": f"seeded Poisson (numpy default_rng, seed {seed:#x})"}
+    # (1) the headline shape: N=2^16, L=24, dnum=3, K=8, key switches.
+    prm = synthetic_params(N, LEVEL, K_P, DNUM)
+    w = Workload(nb, prm, device, seed)
+    head = []
+    rates = sorted({round(plain_value * f) for f in (0.5, 0.9, 1.3)} | {round(batched_value * 0.9)})
+    for rate in rates:
+        row = {}
+        for name, lanes, mb in (("served", 2, BATCH), ("plain", 1, 1)):
+            srv = nb.Server(device=device, lanes=lanes, max_batch=mb, hbm_budget_bytes=budget)
+            count = max(64, min(400, int(rate * 0.12)))
+            jobs = [(w.ctx, w.request(nb, LEVEL, "switch", 0, i)) for i in range(count)]
+            serve_poisson(nb, srv, jobs[:16], rate, seed + 1)  # warm-up
+            row[name] = serve_poisson(nb, srv, jobs, rate, seed)
+            srv.close()
+        head.append(row)
+    out["headline"] = {"workload": "key switches at N=2^16, L=24 (55-bit), K=8 (60-bit), dnum=3",
+                       "rates": head}
+    w.ctx.close()
+    del w
+    # (2) the mixed serving workload: N in 2^13..2^16, dnum in {2,3,4}, L in 4..32, K = alpha = ceil(32/dnum),
+    #     key switch / relinearize / rotate by +-1..+-64.
+    works = {}
+    for logn in (13, 14, 15, 16):
+        for dnum in (2, 3, 4):
+            alpha = -(-32 // dnum)
+            works[(logn, dnum)] = Workload(nb, synthetic_params(1 << logn, 32, alpha, dnum), device,
+                                           seed + 97 * logn + dnum, ring=80)
+    keys = list(works)
+    kinds = ("switch", "relin", "rotate")
+
+    def mixed_jobs(count, s):
+        r = np.random.default_rng(s)
+        jobs = []
+        for i in range(count):
+            wk = works[keys[r.integers(len(keys))]]
+            level = int(r.integers(4, 33))
+            kind = kinds[r.integers(3)]
+            step = int(r.integers(1, 65)) * (1 if r.integers(2) else -1)
+            jobs.append((wk.ctx, wk.request(nb, level, kind, step, i)))
+        return jobs
+
+    srv = nb.Server(device=device, lanes=2, max_batch=BATCH, hbm_budget_bytes=budget)
+    burst = mixed_jobs(600, seed + 3)
+    serve_poisson(nb, srv, burst[:40], 1e6, seed + 4)
+    cap = serve_poisson(nb, srv, burst, 1e7, seed + 5)["throughput"]  # saturation: all arrive at once
+    srv.close()
+    mixed = []
+    for frac in (0.5, 0.9):
+        rate = cap * frac
+        row = {}
+        for name, lanes, mb in (("served", 2, BATCH), ("plain", 1, 1)):
+            srv = nb.Server(device=device, lanes=lanes, max_batch=mb, hbm_budget_bytes=budget)
+            jobs = mixed_jobs(max(100, min(600, int(rate * 0.25))), seed + 7)
+            row[name] = serve_poisson(nb, srv, jobs, rate, seed + 8)
+            srv.close()
+        mixed.append(row)
+    out["mixed"] = {"workload": "N in {2^13..2^16}, dnum in {2,3,4}, L uniform in 4..32, K = alpha = ceil(32/dnum), "
+                                "key switch / relinearize / rotate (steps +-1..+-64), uniform residues, resident "
+                                "ciphertexts and keys",
+                    "served_saturation_per_s": cap, "rates": mixed}
+    for wk in works.values():
+        wk.ctx.close()
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -376,6 +520,8 @@ def run_ours(args, rank, world, local):
 
     line["e2e"] = e2e
     line["plain"] = plain
+    if not args.no_serving:
+        line["serving"] = serving_legs(nb, device, value, plain["value"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_single(prm)
     ctx.close()

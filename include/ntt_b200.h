@@ -158,6 +158,93 @@ int ntt_b200_keyswitch_batch(ntt_b200_context ctx, size_t level, size_t batch, u
                              const uint64_t *key_a, const uint64_t *c0, uint32_t automorphism,
                              void *workspace, size_t workspace_bytes, void *stream);
 
+/* One key-switch request of a request list. All pointers are device pointers
+ * on the context's device; every polynomial is evaluation form over the
+ * request's active Q towers ([level][N]).
+ *  - key switch (run_hybrid_core, include/ntt/openfhe_hybrid_adapter.hpp:163-181):
+ *      (out_b, out_a) = KeySwitch(src) with the full-context key (key_b, key_a);
+ *  - rotation (hybrid_rotate, openfhe_hybrid_adapter.hpp:286-305): c0 set, P*c0
+ *      added and the automorphism applied to the extended QP result before ModDown;
+ *  - relinearization (hybrid_relinearize_in_place, openfhe_hybrid_adapter.hpp:244-282):
+ *      add_b / add_a (c0 / c1 of the ciphertext) are added to the outputs; they may
+ *      equal out_b / out_a (in place).
+ * Requests that share src at one level share one digit decomposition (the
+ * hoisted hybrid_rotate_many, openfhe_hybrid_adapter.hpp:309-361). */
+typedef struct ntt_b200_ks_request {
+  const uint64_t *src;
+  uint64_t *out_b;
+  uint64_t *out_a;
+  const uint64_t *key_b;
+  const uint64_t *key_a;
+  const uint64_t *c0;
+  const uint64_t *add_b;
+  const uint64_t *add_a;
+  uint32_t automorphism;
+  uint32_t level;
+} ntt_b200_ks_request;
+
+/* Workspace bytes of ntt_b200_keyswitch_requests for this request list. */
+int ntt_b200_keyswitch_requests_workspace(ntt_b200_context ctx, const ntt_b200_ks_request *reqs,
+                                          size_t count, size_t *bytes);
+/* Key switch a list of requests of mixed levels, keys, rotations and
+ * relinearization addends. Requests are grouped by level (shape class) and
+ * each group of up to 128 runs as one pass of the fused pipeline; each result
+ * equals the request run alone. Outputs must not overlap any other buffer of
+ * the call (except a request's own addend at the same address). The reference
+ * has no batch API: per request this equals its Session chain
+ * (src/resident.cpp:458-617) and run_hybrid_core. */
+int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request *reqs, size_t count,
+                                void *workspace, size_t workspace_bytes, void *stream);
+
+/* Continuous-batching key-switch server. Requests (ntt_b200_ks_request: key
+ * switch, relinearization or rotation) arrive from any host thread and refer to
+ * device-resident ciphertexts and keys that the caller keeps alive until the
+ * ticket completes. A scheduler thread forms waves of the oldest pending
+ * request's (context, level) class, up to max_batch, and launches each on the
+ * first free lane (a CUDA stream) once its workspace fits hbm_budget_bytes next
+ * to the waves in flight: requests arriving while others run join the next
+ * wave as lanes and memory free up, and waves on different lanes overlap on
+ * the device. Each result equals the request run alone. The reference has no
+ * server (one request per Session transaction, src/resident.cpp); admission
+ * follows its Limits/Reservation budget model (src/resident.cpp:10-28). */
+typedef struct ntt_b200_server_s *ntt_b200_server;
+typedef struct ntt_b200_server_config {
+  int device;
+  int lanes;      /* concurrent waves (CUDA streams), 1..16 */
+  int max_batch;  /* requests per wave, 1..1024 */
+  int reserved;
+  size_t hbm_budget_bytes; /* workspace of all in-flight waves */
+} ntt_b200_server_config;
+typedef struct ntt_b200_ticket_info {
+  int status;          /* NTT_B200_OK or the request's error */
+  uint32_t wave_size;  /* requests in the wave that carried it */
+  int lane;
+  int reserved;
+  double queue_us;     /* submission -> wave launch */
+  double latency_us;   /* submission -> GPU completion of its wave */
+} ntt_b200_ticket_info;
+typedef struct ntt_b200_server_report {
+  uint64_t completed, waves;
+  double mean_wave, p50_ms, p99_ms, max_ms;
+  double throughput;   /* completed / (last completion - first submission), per second */
+  size_t peak_bytes, in_flight_bytes;
+} ntt_b200_server_report;
+const char *ntt_b200_server_last_error(void);
+int ntt_b200_server_create(ntt_b200_server *out, const ntt_b200_server_config *cfg);
+/* Validates the request alone (contract errors return here, before queueing). */
+int ntt_b200_server_submit(ntt_b200_server srv, ntt_b200_context ctx, const ntt_b200_ks_request *req,
+                           uint64_t *ticket);
+/* Waits up to timeout_ms: NTT_B200_OK (ticket released), NTT_B200_ERR_TIMEOUT,
+ * or the request's error. */
+int ntt_b200_server_wait(ntt_b200_server srv, uint64_t ticket, uint32_t timeout_ms,
+                         ntt_b200_ticket_info *info);
+/* Waits until nothing is pending or in flight. */
+int ntt_b200_server_drain(ntt_b200_server srv, uint32_t timeout_ms);
+/* Latency percentiles and throughput of completed requests; reset != 0 clears them. */
+int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int reset);
+/* Finishes pending and in-flight work, then frees the server. */
+int ntt_b200_server_destroy(ntt_b200_server srv);
+
 /* MAC with per-digit device pointers (count digits of L+K towers each):
  * full_key_rows != 0 -> key pointers are full-context digits (rows chosen by
  * key_indices); 0 -> keys are already packed active QP rows. accumulate != 0

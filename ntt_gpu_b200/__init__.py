@@ -17,7 +17,8 @@ import os
 
 from .build import LIB
 
-__all__ = ["ContractError", "CudaError", "WorkspaceError", "Context", "library", "load",
+__all__ = ["ContractError", "CudaError", "WorkspaceError", "Context", "KsRequest", "make_request", "Server",
+           "library", "load",
            "kernel_launches", "OP_MOD_UP", "OP_MOD_DOWN", "OP_DIGITS", "OP_KEYSWITCH"]
 
 OK, ERR_CONTRACT, ERR_CUDA, ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_TIMEOUT, NOT_READY = range(7)
@@ -63,6 +64,15 @@ _SIGNATURES = {
     "ntt_b200_keyswitch": ([_P, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
     "ntt_b200_keyswitch_batch": ([_P, _SZ, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
     "ntt_b200_hybrid_mac_digits": ([_P, _SZ, _P, _P, _P, _P, _P, _SZ, _I, _I, _P], _I),
+    "ntt_b200_keyswitch_requests_workspace": ([_P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_keyswitch_requests": ([_P, _P, _SZ, _P, _SZ, _P], _I),
+    "ntt_b200_server_last_error": ([], ctypes.c_char_p),
+    "ntt_b200_server_create": ([ctypes.POINTER(_P), _P], _I),
+    "ntt_b200_server_submit": ([_P, _P, _P, ctypes.POINTER(_U64)], _I),
+    "ntt_b200_server_wait": ([_P, _U64, ctypes.c_uint32, _P], _I),
+    "ntt_b200_server_drain": ([_P, ctypes.c_uint32], _I),
+    "ntt_b200_server_stats": ([_P, _P, _I], _I),
+    "ntt_b200_server_destroy": ([_P], _I),
     "ntt_b200_stream_create": ([_I, ctypes.POINTER(_P)], _I),
     "ntt_b200_stream_destroy": ([_P], _I),
     "ntt_b200_stream_synchronize": ([_P], _I),
@@ -80,6 +90,33 @@ _SIGNATURES = {
     "ntt_b200_timing_reset": ([], _I),
     "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),
 }
+
+
+class KsRequest(ctypes.Structure):
+    """ntt_b200_ks_request: one key-switch / rotation / relinearization request."""
+    _fields_ = [("src", _P), ("out_b", _P), ("out_a", _P), ("key_b", _P), ("key_a", _P), ("c0", _P),
+                ("add_b", _P), ("add_a", _P), ("automorphism", ctypes.c_uint32), ("level", ctypes.c_uint32)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", _I), ("lanes", _I), ("max_batch", _I), ("reserved", _I), ("hbm_budget_bytes", _SZ)]
+
+
+class TicketInfo(ctypes.Structure):
+    _fields_ = [("status", _I), ("wave_size", ctypes.c_uint32), ("lane", _I), ("reserved", _I),
+                ("queue_us", ctypes.c_double), ("latency_us", ctypes.c_double)]
+
+
+class ServerReport(ctypes.Structure):
+    _fields_ = [("completed", _U64), ("waves", _U64), ("mean_wave", ctypes.c_double), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("throughput", ctypes.c_double),
+                ("peak_bytes", _SZ), ("in_flight_bytes", _SZ)]
+
+
+def make_request(level, src, out_b, out_a, key_b, key_a, c0=None, automorphism=0, add_b=None, add_a=None):
+    """A KsRequest from torch CUDA tensors (None for the optional ones)."""
+    return KsRequest(_ptr(src), _ptr(out_b), _ptr(out_a), _ptr(key_b), _ptr(key_a), _ptr(c0), _ptr(add_b),
+                     _ptr(add_a), int(automorphism), int(level))
 
 
 def load(path: str = LIB):
@@ -106,10 +143,11 @@ def kernel_launches() -> int:
     return int(load().ntt_b200_kernel_launches())
 
 
-def _check(rc: int):
+def _check(rc: int, server: bool = False):
     if rc == OK:
         return
-    msg = load().ntt_b200_last_error().decode()
+    lib = load()
+    msg = (lib.ntt_b200_server_last_error() if server else lib.ntt_b200_last_error()).decode()
     if rc == ERR_CONTRACT or rc == ERR_UNSUPPORTED:
         raise ContractError(msg)
     if rc == ERR_WORKSPACE:
@@ -243,6 +281,22 @@ class Context:
                                                   _ptr(key_b), _ptr(key_a), _ptr(c0), automorphism,
                                                   _ptr(workspace), workspace.numel() * 8, _stream(stream)))
 
+    def requests_workspace_bytes(self, reqs) -> int:
+        arr = (KsRequest * len(reqs))(*reqs)
+        out = _SZ()
+        _check(self._lib.ntt_b200_keyswitch_requests_workspace(self._h, arr, len(reqs), ctypes.byref(out)))
+        return out.value
+
+    def requests_workspace(self, reqs):
+        import torch
+        nbytes = self.requests_workspace_bytes(reqs)
+        return torch.empty(max(1, (nbytes + 7) // 8), dtype=torch.int64, device=f"cuda:{self.device}")
+
+    def keyswitch_requests(self, reqs, workspace, stream=None):
+        arr = (KsRequest * len(reqs))(*reqs)
+        _check(self._lib.ntt_b200_keyswitch_requests(self._h, arr, len(reqs), _ptr(workspace),
+                                                     workspace.numel() * 8, _stream(stream)))
+
     def keyswitch(self, level, out_b, out_a, src, key_b, key_a, workspace, c0=None, automorphism=0,
                   stream=None):
         _check(self._lib.ntt_b200_keyswitch(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(src), _ptr(key_b),
@@ -250,8 +304,53 @@ class Context:
                                             workspace.numel() * 8, _stream(stream)))
 
 
+class Server:
+    """Continuous-batching key-switch server (ntt_b200_server_*).
+
+    submit() takes a KsRequest over device-resident buffers (kept alive by the
+    caller until wait() returns) and returns a ticket; wait() blocks until the
+    request's wave finished on the GPU and returns its TicketInfo.
+    """
+
+    def __init__(self, device=0, lanes=2, max_batch=16, hbm_budget_bytes=8 << 30):
+        self._lib = load()
+        cfg = ServerConfig(int(device), int(lanes), int(max_batch), 0, int(hbm_budget_bytes))
+        h = _P()
+        _check(self._lib.ntt_b200_server_create(ctypes.byref(h), ctypes.byref(cfg)), server=True)
+        self._h = h
+
+    def submit(self, ctx: "Context", req: KsRequest) -> int:
+        t = _U64()
+        _check(self._lib.ntt_b200_server_submit(self._h, ctx._h, ctypes.byref(req), ctypes.byref(t)), server=True)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> TicketInfo:
+        info = TicketInfo()
+        _check(self._lib.ntt_b200_server_wait(self._h, ticket, timeout_ms, ctypes.byref(info)), server=True)
+        return info
+
+    def drain(self, timeout_ms: int = 120000):
+        _check(self._lib.ntt_b200_server_drain(self._h, timeout_ms), server=True)
+
+    def stats(self, reset=False) -> dict:
+        st = ServerReport()
+        _check(self._lib.ntt_b200_server_stats(self._h, ctypes.byref(st), int(reset)), server=True)
+        return {f: getattr(st, f) for f, _ in ServerReport._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(self._lib.ntt_b200_server_destroy(self._h), server=True)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col", "ntt_small", "conv", "mac",
-                  "rotate", "correct", "pointwise")
+                  "rotate", "correct", "pointwise", "table")
 
 
 def timing_enable(on: bool = True):

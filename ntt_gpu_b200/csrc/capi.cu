@@ -326,6 +326,8 @@ struct Slot {
 struct NttFinal {
   u64 *dst = nullptr, *dst_odd = nullptr;
   u64 stride = 0;
+  u64 *const *dst_list = nullptr;        // per-polynomial destinations (device array)
+  const u64 *const *add_list = nullptr;  // per-polynomial addends (device array; entries may be null)
   const u64 *epi_left = nullptr;
   u64 epi_left_stride = 0;
   const b200::Shoup *epi_pinv = nullptr;
@@ -382,10 +384,13 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
   b200::NttBatch second = b;
   second.src = b.dst;
   second.src_stride = b.dst_stride;
+  second.src_list = nullptr;
   if (fin) {
     second.dst = fin->dst;
     second.dst_odd = fin->dst_odd;
     second.dst_stride = fin->stride;
+    second.dst_list = fin->dst_list;
+    second.add_list = fin->add_list;
     second.epi_left = fin->epi_left;
     second.epi_left_stride = fin->epi_left_stride;
     second.epi_pinv = fin->epi_pinv;
@@ -448,8 +453,10 @@ dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
 // polynomials with separate source and destination strides (words). `fin`
 // (forward only) redirects the final pass: split destination and/or the ModDown
 // epilogue (left - x) * P^-1; small transforms run it as a separate kernel.
+// src_list (device array, one entry per polynomial) replaces src / src_stride.
 void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots, size_t polys,
-             u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr) {
+             u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr,
+             const u64 *const *src_list = nullptr) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   require(!fin || !inverse, "final-pass redirection is forward only");
   for (size_t first = 0; first < slots.size(); first += b200::kMaxSlots) {
@@ -463,6 +470,7 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
     }
     b.src = src;
     b.dst = dst;
+    b.src_list = src_list;
     if (c.logn <= 11) {
       const dim3 grid(1, (unsigned)count, (unsigned)polys);
       const int threads = std::min<int>(b200::kNttThreads, std::max<int>(32, (int)(c.n / 2)));
@@ -479,6 +487,8 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
         b200::CorrectArgs a{};
         a.dst = fin->dst;
         a.dst_odd = fin->dst_odd;
+        a.dst_list = fin->dst_list;
+        a.add_list = fin->add_list;
         a.left = fin->epi_left;
         a.right = dst;
         a.pinv = fin->epi_pinv;
@@ -595,8 +605,11 @@ Carver carve(const Ctx &c, void *ws, size_t bytes, int op, size_t level, size_t 
 // ---- composite operations over a batch of polynomials ----------------------------------
 // ModDown of `polys` evaluation-QP polynomials (stride src_stride) into
 // evaluation Q_L (stride dst_stride, or split even/odd destinations).
+// dst_list / add_list (device arrays, one entry per polynomial) optionally
+// redirect each output and add a per-polynomial addend.
 void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst_stride, const u64 *src,
-                 u64 src_stride, Carver &ws, cudaStream_t st) {
+                 u64 src_stride, Carver &ws, cudaStream_t st, u64 *const *dst_list = nullptr,
+                 const u64 *const *add_list = nullptr) {
   const size_t n = c.n, K = c.k;
   u64 *p_coeff = ws.take(polys * K * n);
   u64 *corr = ws.take(polys * L * n);
@@ -610,6 +623,8 @@ void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst
   fin.dst = dst;
   fin.dst_odd = dst_odd;
   fin.stride = dst_stride;
+  fin.dst_list = dst_list;
+  fin.add_list = add_list;
   fin.epi_left = src;
   fin.epi_left_stride = src_stride;
   fin.epi_pinv = c.down_plan(L)->p_inv;
@@ -619,13 +634,15 @@ void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst
 // Hybrid digits of `polys` evaluation-Q_L inputs (stride L*n) into digits
 // (stride beta*T*n). copy_own = false leaves each digit's own towers unwritten
 // (the fused MAC reads them from the input).
+// src_list (device array, one input per polynomial) replaces the strided src.
 void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carver &ws, bool copy_own,
-               cudaStream_t st) {
+               cudaStream_t st, const u64 *const *src_list = nullptr) {
   const size_t n = c.n, K = c.k, T = L + K;
   const size_t beta = 1 + (L - 1) / c.alpha;
   const u64 dstride = beta * T * n;
+  require(!(copy_own && src_list), "own-tower copies need a strided source");
   u64 *coeff = ws.take(polys * L * n);
-  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), polys, L * n, L * n, true, st);
+  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), polys, L * n, L * n, true, st, nullptr, src_list);
   const auto all = qp_ids(c, L);
   std::vector<Slot> fwd;
   size_t digit = 0;
@@ -654,21 +671,26 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
 void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride,
             const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
             const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a, bool full_key_rows,
-            bool accumulate, cudaStream_t st) {
+            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr) {
   const size_t n = c.n, T = L + c.k;
   const size_t beta = digits.size();
-  require(beta >= 1 && beta <= (size_t)b200::kMaxDigits && key_b.size() == beta && key_a.size() == beta,
+  require(beta >= 1 && beta <= (size_t)b200::kMaxDigits &&
+              (req || (key_b.size() == beta && key_a.size() == beta)),
           "MAC digit count out of range");
   b200::MacArgs a{};
   a.out_b = out_b;
   a.out_a = out_a;
   for (size_t d = 0; d < beta; ++d) {
     a.digit[d] = digits[d];
-    a.key_b[d] = key_b[d];
-    a.key_a[d] = key_a[d];
+    if (!req) {
+      a.key_b[d] = key_b[d];
+      a.key_a[d] = key_a[d];
+    }
   }
   a.input = input;
   a.tc = c.d_tc;
+  a.req = req;
+  a.key_digit_stride = c.towers() * n;
   a.poly_stride_out = out_stride;
   a.poly_stride_digits = digit_poly_stride;
   a.poly_stride_input = L * n;
@@ -717,8 +739,9 @@ std::vector<const u64 *> key_digits(const Ctx &c, const u64 *key, size_t beta) {
 }
 
 void do_rotate(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,
-               u64 stride, const u64 *c0, u64 c0_stride, uint32_t g, cudaStream_t st) {
-  require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
+               u64 stride, const u64 *c0, u64 c0_stride, uint32_t g, cudaStream_t st,
+               const b200::ReqDesc *req = nullptr) {
+  require(req || ((g & 1) && g < 2 * c.n), "invalid negacyclic automorphism index");
   b200::RotateArgs a{};
   a.out_b = out_b;
   a.out_a = out_a;
@@ -727,6 +750,7 @@ void do_rotate(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, const u64
   a.c0 = c0;
   a.plan = c.down_plan(L);
   a.tc = c.d_tc;
+  a.req = req;
   a.poly_stride = stride;
   a.c0_poly_stride = c0_stride;
   a.level = (int)L;
@@ -758,6 +782,177 @@ void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const 
     ext = rot;
   }
   do_mod_down(c, L, 2 * batch, out_b, out_a, L * n, ext, T * n, ws, st);
+}
+
+// ---- request-table key switch --------------------------------------------------------
+// Requests of one call are grouped by level (a shape class) and cut into chunks
+// of at most kMaxGroup. Each chunk is one pass of the fused pipeline; every
+// kernel reads its request's pointers from a small device table, so a chunk
+// mixes keys, rotations, relinearization addends and callers' buffers freely.
+// Requests of a chunk that share an input share its digits (the hoisted
+// decomposition of the reference's hybrid_rotate_many,
+// include/ntt/openfhe_hybrid_adapter.hpp:309-361).
+constexpr size_t kMaxGroup = 128;
+
+struct Chunk {
+  size_t level = 0;
+  std::vector<size_t> idx;          // request indices, call order
+  std::vector<const u64 *> usrc;    // unique inputs, first-seen order
+  std::vector<uint32_t> dslot;      // per request: index into usrc
+  bool rotate = false, add = false;
+};
+
+std::vector<Chunk> plan_chunks(const ntt_b200_ks_request *reqs, size_t count) {
+  std::vector<size_t> levels;
+  for (size_t i = 0; i < count; ++i)
+    if (std::find(levels.begin(), levels.end(), (size_t)reqs[i].level) == levels.end())
+      levels.push_back(reqs[i].level);
+  std::vector<Chunk> out;
+  for (size_t L : levels) {
+    Chunk cur;
+    auto flush = [&] {
+      if (!cur.idx.empty()) out.push_back(std::move(cur));
+      cur = Chunk{};
+    };
+    for (size_t i = 0; i < count; ++i) {
+      if ((size_t)reqs[i].level != L) continue;
+      if (cur.idx.size() == kMaxGroup) flush();
+      cur.level = L;
+      const u64 *src = reqs[i].src;
+      auto it = std::find(cur.usrc.begin(), cur.usrc.end(), src);
+      uint32_t slot = (uint32_t)(it - cur.usrc.begin());
+      if (it == cur.usrc.end()) cur.usrc.push_back(src);
+      cur.idx.push_back(i);
+      cur.dslot.push_back(slot);
+      cur.rotate = cur.rotate || reqs[i].c0 != nullptr;
+      cur.add = cur.add || reqs[i].add_b != nullptr || reqs[i].add_a != nullptr;
+    }
+    flush();
+  }
+  return out;
+}
+
+// Words of a chunk's device table: ReqDesc[r] | usrc[u] | dst_list[2r] | add_list[2r].
+size_t table_words(size_t r, size_t u) { return 6 * r + u + 4 * r; }
+
+size_t chunk_bytes(const Ctx &c, const Chunk &ch) {
+  const size_t n = c.n, L = ch.level, K = c.k, T = L + K, r = ch.idx.size(), u = ch.usrc.size();
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  return aligned_bytes(table_words(r, u)) + aligned_bytes(u * beta * T * n) + aligned_bytes(u * L * n) +
+         aligned_bytes(2 * r * T * n) + (ch.rotate ? aligned_bytes(2 * r * T * n) : 0) +
+         aligned_bytes(2 * r * K * n) + aligned_bytes(2 * r * L * n);
+}
+
+template <int W>
+void put_table_t(const std::vector<u64> &words, u64 *dst, cudaStream_t st) {
+  b200::Words<W> p;
+  p.count = (uint32_t)words.size();
+  std::memcpy(p.w, words.data(), words.size() * sizeof(u64));
+  Timed t("table", st);
+  b200::put_words<W><<<1, 256, 0, st>>>(p, dst);
+  t.done();
+}
+void put_table(const std::vector<u64> &words, u64 *dst, cudaStream_t st) {
+  if (words.size() <= 256) put_table_t<256>(words, dst, st);
+  else if (words.size() <= 1024) put_table_t<1024>(words, dst, st);
+  else if (words.size() <= 2048) put_table_t<2048>(words, dst, st);
+  else throw ContractError("request table too large");
+}
+
+u64 as_word(const void *p) { return (u64)reinterpret_cast<uintptr_t>(p); }
+
+void run_chunk(Ctx &c, const ntt_b200_ks_request *reqs, const Chunk &ch, Carver &ws, cudaStream_t st) {
+  const size_t n = c.n, L = ch.level, T = L + c.k, r = ch.idx.size(), u = ch.usrc.size();
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  u64 *table = ws.take(table_words(r, u));
+  std::vector<u64> words;
+  words.reserve(table_words(r, u));
+  for (size_t j = 0; j < r; ++j) {
+    const ntt_b200_ks_request &q = reqs[ch.idx[j]];
+    words.push_back(as_word(q.src));
+    words.push_back(as_word(q.key_b));
+    words.push_back(as_word(q.key_a));
+    words.push_back(as_word(q.c0));
+    words.push_back((u64)(q.c0 ? q.automorphism : 1u) | ((u64)ch.dslot[j] << 32));
+    words.push_back(0);
+  }
+  for (const u64 *p : ch.usrc) words.push_back(as_word(p));
+  for (size_t j = 0; j < r; ++j) {
+    words.push_back(as_word(reqs[ch.idx[j]].out_b));
+    words.push_back(as_word(reqs[ch.idx[j]].out_a));
+  }
+  for (size_t j = 0; j < r; ++j) {
+    words.push_back(as_word(reqs[ch.idx[j]].add_b));
+    words.push_back(as_word(reqs[ch.idx[j]].add_a));
+  }
+  put_table(words, table, st);
+  const auto *desc = reinterpret_cast<const b200::ReqDesc *>(table);
+  const auto *usrc = reinterpret_cast<const u64 *const *>(table + 6 * r);
+  auto *dst_list = reinterpret_cast<u64 *const *>(table + 6 * r + u);
+  const auto *add_list = reinterpret_cast<const u64 *const *>(table + 6 * r + u + 2 * r);
+
+  u64 *digits = ws.take(u * beta * T * n);
+  u64 *acc = ws.take(2 * r * T * n);  // [request][b|a][T][N]
+  u64 *rot = ch.rotate ? ws.take(2 * r * T * n) : nullptr;
+  do_digits(c, L, u, digits, nullptr, ws, false, st, usrc);
+  std::vector<const u64 *> dptr;
+  for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
+  do_mac(c, L, r, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, nullptr, {}, {}, true, false, st, desc);
+  const u64 *ext = acc;
+  if (ch.rotate) {
+    do_rotate(c, L, r, rot, rot + T * n, acc, acc + T * n, 2 * T * n, nullptr, 0, 1, st, desc);
+    ext = rot;
+  }
+  do_mod_down(c, L, 2 * r, nullptr, nullptr, 0, ext, T * n, ws, st, dst_list, ch.add ? add_list : nullptr);
+}
+
+// Host-side checks of a request list, all before anything is enqueued.
+void validate_requests(const Ctx &c, const ntt_b200_ks_request *reqs, size_t count) {
+  require(reqs != nullptr && count >= 1, "empty request list");
+  require(c.k > 0, "QP requires P towers");
+  require(c.k <= 40, "conversion requires 1..40 active Q and P towers");
+  struct Span {
+    uintptr_t lo, hi;
+    size_t req;
+    int role;  // 0 input, 1 out_b, 2 out_a, 3 add_b, 4 add_a
+  };
+  std::vector<Span> spans;
+  const size_t key_words = (1 + (c.m - 1) / c.alpha) * c.towers() * c.n;
+  for (size_t i = 0; i < count; ++i) {
+    const ntt_b200_ks_request &q = reqs[i];
+    require(q.level >= 1 && q.level <= c.m && q.level <= 40, "invalid active Q count");
+    require(q.src && q.out_b && q.out_a && q.key_b && q.key_a, "null pointer");
+    require_aligned({q.src, q.out_b, q.out_a, q.key_b, q.key_a, q.c0, q.add_b, q.add_a});
+    if (q.c0) require((q.automorphism & 1) && q.automorphism < 2 * c.n, "invalid negacyclic automorphism index");
+    const size_t poly = q.level * c.n * sizeof(u64);
+    auto add = [&](const void *p, size_t bytes, int role) {
+      if (p) spans.push_back({reinterpret_cast<uintptr_t>(p), reinterpret_cast<uintptr_t>(p) + bytes, i, role});
+    };
+    add(q.src, poly, 0);
+    add(q.c0, poly, 0);
+    add(q.key_b, key_words * sizeof(u64), 0);
+    add(q.key_a, key_words * sizeof(u64), 0);
+    add(q.out_b, poly, 1);
+    add(q.out_a, poly, 2);
+    add(q.add_b, poly, 3);
+    add(q.add_a, poly, 4);
+  }
+  // Outputs overlap nothing, except a request's own addend at the same address
+  // (in-place relinearization).
+  for (const Span &o : spans) {
+    if (o.role != 1 && o.role != 2) continue;
+    for (const Span &x : spans) {
+      if (&x == &o || x.hi <= o.lo || o.hi <= x.lo) continue;
+      const bool own_addend = x.req == o.req && x.role == o.role + 2 && x.lo == o.lo && x.hi == o.hi;
+      require(own_addend, "a request output overlaps another buffer of the call");
+    }
+  }
+}
+
+size_t requests_bytes(const Ctx &c, const std::vector<Chunk> &chunks) {
+  size_t need = 0;
+  for (const Chunk &ch : chunks) need = std::max(need, chunk_bytes(c, ch));
+  return need;
 }
 }  // namespace
 
@@ -1122,6 +1317,40 @@ int ntt_b200_keyswitch_batch(ntt_b200_context ctx, size_t level, size_t batch, u
     Carver ws = carve(c, workspace, workspace_bytes, NTT_B200_OP_KEYSWITCH, level, batch);
     DeviceGuard guard(c.device);
     do_keyswitch(c, level, batch, out_b, out_a, src, key_b, key_a, c0, automorphism, ws, as_stream(stream));
+  });
+}
+
+int ntt_b200_keyswitch_requests_workspace(ntt_b200_context ctx, const ntt_b200_ks_request *reqs,
+                                          size_t count, size_t *bytes) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(bytes != nullptr, "null output");
+    validate_requests(*ctx, reqs, count);
+    *bytes = requests_bytes(*ctx, plan_chunks(reqs, count));
+  });
+}
+
+int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request *reqs, size_t count,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    Ctx &c = *ctx;
+    validate_requests(c, reqs, count);
+    require_aligned({workspace});
+    const auto chunks = plan_chunks(reqs, count);
+    const size_t need = requests_bytes(c, chunks);
+    if (!workspace || workspace_bytes < need) throw WorkspaceError("workspace missing or too small");
+    DeviceGuard guard(c.device);
+    for (const Chunk &ch : chunks) {
+      c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, ch.level));
+      c.down_plan(ch.level);
+    }
+    const cudaStream_t st = as_stream(stream);
+    for (const Chunk &ch : chunks) {
+      // Chunks run in stream order, so each reuses the same workspace.
+      Carver ws{reinterpret_cast<char *>(workspace), workspace_bytes};
+      run_chunk(c, reqs, ch, ws, st);
+    }
   });
 }
 

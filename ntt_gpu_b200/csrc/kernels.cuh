@@ -83,6 +83,8 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
 // ---- ModDown tail: (l - r) * [P^-1]_q  (resident_conversion.hpp:45-49) ---------
 struct CorrectArgs {
   u64 *dst, *dst_odd;  // dst_odd set: polynomial z writes (z odd ? dst_odd : dst) + (z / 2) * stride
+  u64 *const *dst_list;        // optional: polynomial z writes dst_list[z]
+  const u64 *const *add_list;  // optional: add_list[z] (if not null) is added to the result
   const u64 *left, *right;
   const Shoup *pinv;  // [P^-1]_q by Q tower
   const TowerConsts *tc;
@@ -99,9 +101,13 @@ __global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
   const u64 z = blockIdx.z;
   const u64 l = a.left[z * a.poly_stride_left + t * n + i];
   const u64 r = a.right[z * a.poly_stride_right + t * n + i];
-  u64 *dst = a.dst_odd ? ((z & 1) ? a.dst_odd : a.dst) + (z >> 1) * a.poly_stride_dst
-                       : a.dst + z * a.poly_stride_dst;
-  dst[t * n + i] = shoup_canon(sub_mod(l, r, q), pinv.w, pinv.wq, q);
+  u64 *dst = a.dst_list ? a.dst_list[z]
+             : a.dst_odd ? ((z & 1) ? a.dst_odd : a.dst) + (z >> 1) * a.poly_stride_dst
+                         : a.dst + z * a.poly_stride_dst;
+  u64 o = shoup_canon(sub_mod(l, r, q), pinv.w, pinv.wq, q);
+  const u64 *add = a.add_list ? a.add_list[z] : nullptr;
+  if (add) o = add_mod(o, add[t * n + i], q);
+  dst[t * n + i] = o;
 }
 
 // ---- Hybrid MAC over all digits in one pass --------------------------------------
@@ -112,16 +118,53 @@ __global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
 // With accumulate set, the result is added to the existing outputs (the
 // reference's per-digit primitive for digits after the first).
 constexpr int kMaxDigits = 40;
+
+// One key-switch request of a request-table launch (a device-resident table
+// written by put_words before the pipeline runs).
+struct ReqDesc {
+  const u64 *src;            // evaluation Q_L component being switched ([L][N])
+  const u64 *key_b, *key_a;  // full-context key: digit d at key + d * key_digit_stride
+  const u64 *c0;             // rotation: first component ([L][N]); null: no rotation
+  uint32_t g;                // automorphism index (1 = identity)
+  uint32_t dslot;            // digit slot; requests that share an input share its digits
+  u64 pad;
+};
+static_assert(sizeof(ReqDesc) == 48, "ReqDesc is uploaded as 6 words");
+
 struct MacArgs {
   u64 *out_b, *out_a;
   const u64 *digit[kMaxDigits];  // digit d, tower t at digit[d] + z * poly_stride_digits + t * n
   const u64 *key_b[kMaxDigits], *key_a[kMaxDigits];
   const u64 *input;              // if set: digit d's own Q towers are read from input + t * n
   const TowerConsts *tc;
+  const ReqDesc *req;            // if set: per-request input, keys and digit slot (full-context keys)
+  u64 key_digit_stride;          // words between key digits (request-table mode)
   u64 poly_stride_out, poly_stride_digits, poly_stride_input;
   int level, m, beta, alpha, logn;
   bool full_key_rows, accumulate;
 };
+
+// Per-request bases of a MAC thread: request z's digit slot, input and keys.
+struct MacBases {
+  u64 dz;
+  const u64 *input;
+  const u64 *kb, *ka;  // request-table mode: digit 0 of the request's key
+};
+__device__ __forceinline__ MacBases mac_bases(const MacArgs &a, u64 z) {
+  MacBases m;
+  if (a.req) {
+    const ReqDesc r = a.req[z];
+    m.dz = r.dslot;
+    m.input = r.src;
+    m.kb = r.key_b;
+    m.ka = r.key_a;
+  } else {
+    m.dz = z;
+    m.input = a.input ? a.input + z * a.poly_stride_input : nullptr;
+    m.kb = m.ka = nullptr;
+  }
+  return m;
+}
 // Grid: x = coefficient block, y = request, z = QP tower. Requests vary faster
 // than towers, so the key rows of one tower stay in L2 while every request of
 // the batch streams through them.
@@ -134,16 +177,19 @@ __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
   if (i >= n) return;
   const int g = t < a.level ? t : a.m + (t - a.level);
   const Reducer red = a.tc[g].red;
-  const u64 row = a.full_key_rows ? u64(g) : u64(t);
-  const int own = (a.input && t < a.level) ? t / a.alpha : -1;
-  const u64 doff = z * a.poly_stride_digits + t * n + i;
+  const u64 row = (a.full_key_rows || a.req) ? u64(g) : u64(t);
+  const MacBases mb = mac_bases(a, z);
+  const int own = (mb.input && t < a.level) ? t / a.alpha : -1;
+  const u64 doff = mb.dz * a.poly_stride_digits + t * n + i;
   using Acc = typename std::conditional<WIDE, Acc192, Acc128>::type;
   Acc ab{}, aa{};
 #pragma unroll 4
   for (int j = 0; j < a.beta; ++j) {
-    const u64 x = j == own ? a.input[z * a.poly_stride_input + t * n + i] : a.digit[j][doff];
-    acc_mad(ab, x, a.key_b[j][row * n + i]);
-    acc_mad(aa, x, a.key_a[j][row * n + i]);
+    const u64 x = j == own ? mb.input[t * n + i] : a.digit[j][doff];
+    const u64 *kb = a.req ? mb.kb + j * a.key_digit_stride : a.key_b[j];
+    const u64 *ka = a.req ? mb.ka + j * a.key_digit_stride : a.key_a[j];
+    acc_mad(ab, x, kb[row * n + i]);
+    acc_mad(aa, x, ka[row * n + i]);
   }
   const u64 o = z * a.poly_stride_out + t * n + i;
   u64 rb = reduce(ab, red), ra = reduce(aa, red);
@@ -166,17 +212,20 @@ __global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
   if (i >= n) return;
   const int g = t < a.level ? t : a.m + (t - a.level);
   const Reducer red = a.tc[g].red;
-  const u64 row = a.full_key_rows ? u64(g) : u64(t);
-  const int own = (a.input && t < a.level) ? t / a.alpha : -1;
-  const u64 doff = z * a.poly_stride_digits + t * n + i;
+  const u64 row = (a.full_key_rows || a.req) ? u64(g) : u64(t);
+  const MacBases mb = mac_bases(a, z);
+  const int own = (mb.input && t < a.level) ? t / a.alpha : -1;
+  const u64 doff = mb.dz * a.poly_stride_digits + t * n + i;
   using Acc = typename std::conditional<WIDE, Acc192, Acc128>::type;
   Acc b0{}, b1{}, a0{}, a1{};
 #pragma unroll
   for (int j = 0; j < BETA; ++j) {
-    const ulonglong2 x = j == own ? *reinterpret_cast<const ulonglong2 *>(a.input + z * a.poly_stride_input + t * n + i)
+    const ulonglong2 x = j == own ? *reinterpret_cast<const ulonglong2 *>(mb.input + t * n + i)
                                   : *reinterpret_cast<const ulonglong2 *>(a.digit[j] + doff);
-    const ulonglong2 kb = *reinterpret_cast<const ulonglong2 *>(a.key_b[j] + row * n + i);
-    const ulonglong2 ka = *reinterpret_cast<const ulonglong2 *>(a.key_a[j] + row * n + i);
+    const u64 *kbp = a.req ? mb.kb + j * a.key_digit_stride : a.key_b[j];
+    const u64 *kap = a.req ? mb.ka + j * a.key_digit_stride : a.key_a[j];
+    const ulonglong2 kb = *reinterpret_cast<const ulonglong2 *>(kbp + row * n + i);
+    const ulonglong2 ka = *reinterpret_cast<const ulonglong2 *>(kap + row * n + i);
     acc_mad(b0, x.x, kb.x);
     acc_mad(b1, x.y, kb.y);
     acc_mad(a0, x.x, ka.x);
@@ -208,11 +257,14 @@ __device__ __forceinline__ uint32_t automorphism_source(uint32_t k, int logn, ui
   const uint32_t src = (uint32_t)((u64(odd) * g) & ((u64(2) << logn) - 1));
   return __brev(src >> 1) >> (32 - logn);
 }
+// With a request table, request z rotates by req[z].g and adds P * req[z].c0
+// (a request without c0 and g = 1 passes through unchanged).
 struct RotateArgs {
   u64 *out_b, *out_a;
   const u64 *ext_b, *ext_a, *c0;
   const DownPlan *plan;
   const TowerConsts *tc;
+  const ReqDesc *req;
   u64 poly_stride, c0_poly_stride;
   int level, m, logn;
   uint32_t g;
@@ -223,15 +275,35 @@ __global__ void __launch_bounds__(kEwThreads) rotate_kernel(RotateArgs a) {
   const int t = blockIdx.y;
   if (k >= n) return;
   const u64 z = blockIdx.z;
-  const u64 src = t * n + automorphism_source((uint32_t)k, a.logn, a.g);
+  uint32_t g = a.g;
+  const u64 *c0 = a.c0 ? a.c0 + z * a.c0_poly_stride : nullptr;
+  if (a.req) {
+    g = a.req[z].g;
+    c0 = a.req[z].c0;
+  }
+  const u64 src = t * n + automorphism_source((uint32_t)k, a.logn, g);
   u64 b = a.ext_b[z * a.poly_stride + src];
-  if (t < a.level) {
+  if (c0 && t < a.level) {
     const u64 q = a.tc[t].q;
     const Shoup pm = a.plan->p_mod[t];
-    b = add_mod(b, shoup_canon(a.c0[z * a.c0_poly_stride + src], pm.w, pm.wq, q), q);
+    b = add_mod(b, shoup_canon(c0[src], pm.w, pm.wq, q), q);
   }
   a.out_b[z * a.poly_stride + t * n + k] = b;
   a.out_a[z * a.poly_stride + t * n + k] = a.ext_a[z * a.poly_stride + src];
+}
+
+// ---- request-table upload ------------------------------------------------------------
+// Copies a small table from the launch's parameter space into device memory,
+// so a host-built table reaches the GPU in stream order without a host staging
+// buffer.
+template <int WORDS>
+struct Words {
+  uint32_t count;
+  u64 w[WORDS];
+};
+template <int WORDS>
+__global__ void put_words(Words<WORDS> p, u64 *dst) {
+  for (uint32_t i = threadIdx.x; i < p.count; i += blockDim.x) dst[i] = p.w[i];
 }
 
 // ---- pointwise product ------------------------------------------------------------

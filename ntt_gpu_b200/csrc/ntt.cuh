@@ -38,18 +38,36 @@ constexpr int kRowPad = 272;  // 256 words + one pad word per 16
 // key switch land in separate caller buffers).
 // Optional forward epilogue (ModDown tail, include/ntt/resident_conversion.hpp:45-49):
 // with epi_left set, the last forward pass writes (left - ntt(x)) * pinv[id].
+// Optional per-polynomial pointer lists (device arrays indexed by z) replace
+// the strided bases: src_list[z] / dst_list[z] are polynomial z's source and
+// destination, and add_list[z] (entries may be null) is added to the ModDown
+// epilogue's output (relinearization: c0 + b, c1 + a).
 constexpr int kMaxSlots = 128;
 struct NttBatch {
   u64 *dst;
   const u64 *src;
   u64 src_stride, dst_stride;
   u64 *dst_odd;
+  const u64 *const *src_list;
+  u64 *const *dst_list;
+  const u64 *const *add_list;
   const u64 *epi_left;
   u64 epi_left_stride;
   const Shoup *epi_pinv;
   uint32_t off[kMaxSlots];
   uint16_t id[kMaxSlots];
 };
+
+__device__ __forceinline__ const u64 *poly_src(const NttBatch &b, u64 z) {
+  return b.src_list ? b.src_list[z] : b.src + z * b.src_stride;
+}
+__device__ __forceinline__ u64 *poly_dst(const NttBatch &b, u64 z) {
+  if (b.dst_list) return b.dst_list[z];
+  return b.dst_odd ? ((z & 1) ? b.dst_odd : b.dst) + (z >> 1) * b.dst_stride : b.dst + z * b.dst_stride;
+}
+__device__ __forceinline__ const u64 *poly_add(const NttBatch &b, u64 z) {
+  return b.add_list ? b.add_list[z] : nullptr;
+}
 
 #ifndef NTT_MINB
 #define NTT_MINB 4
@@ -71,8 +89,8 @@ __device__ __forceinline__ TowerView tower_view(const NttBatch &b, const DeviceT
   v.c = T.tc + g;
   v.tw = (inv ? T.inv : T.fwd) + g * n;
   const u64 z = blockIdx.z;
-  v.src = b.src + z * b.src_stride + offset;
-  v.dst = (b.dst_odd ? ((z & 1) ? b.dst_odd : b.dst) + (z >> 1) * b.dst_stride : b.dst + z * b.dst_stride) + offset;
+  v.src = poly_src(b, z) + offset;
+  v.dst = poly_dst(b, z) + offset;
   return v;
 }
 
@@ -300,6 +318,8 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b,
                     row0 * 256;
   const Shoup pinv = b.epi_pinv[b.id[blockIdx.y]];
   u64 *out = v.dst + row0 * 256;
+  const u64 *add = poly_add(b, blockIdx.z);
+  if (add) add += u64(b.off[blockIdx.y]) * (u64(1) << T.logn) + row0 * 256;
   for (int j = threadIdx.x; j < 16 * 128; j += kNttThreads) {
     const int rr = j >> 7, c = (j & 127) * 2;
     const int sidx = rr * kRowPad + pad_col(c);
@@ -307,6 +327,11 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b,
     ulonglong2 o;
     o.x = shoup_canon(sub_mod(l.x, tile[sidx], q), pinv.w, pinv.wq, q);
     o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
+    if (add) {
+      const ulonglong2 e = *reinterpret_cast<const ulonglong2 *>(add + rr * 256 + c);
+      o.x = add_mod(o.x, e.x, q);
+      o.y = add_mod(o.y, e.y, q);
+    }
     *reinterpret_cast<ulonglong2 *>(out + rr * 256 + c) = o;
   }
 }

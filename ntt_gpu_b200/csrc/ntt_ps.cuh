@@ -49,8 +49,8 @@ __device__ __forceinline__ TowerView view_at(const NttBatch &b, const DeviceTabl
   TowerView v;
   v.c = T.tc + g;
   v.tw = (inv ? T.inv : T.fwd) + g * n;
-  v.src = b.src + z * b.src_stride + offset;
-  v.dst = (b.dst_odd ? ((z & 1) ? b.dst_odd : b.dst) + (z >> 1) * b.dst_stride : b.dst + z * b.dst_stride) + offset;
+  v.src = poly_src(b, z) + offset;
+  v.dst = poly_dst(b, z) + offset;
   return v;
 }
 
@@ -330,6 +330,8 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
       // ModDown tail: (left - ntt(x)) * [P^-1]_q.
       const u64 *left = b.epi_left + u64(tc.z) * b.epi_left_stride + u64(b.off[tc.slot]) * N + u64(tc.x) * kTileWords;
       const Shoup pinv = b.epi_pinv[b.id[tc.slot]];
+      const u64 *add = poly_add(b, tc.z);
+      if (add) add += u64(b.off[tc.slot]) * N + u64(tc.x) * kTileWords;
       for (int j = threadIdx.x; j < kTileWords / 2; j += kNttThreads) {
         const int rr = j >> 7, chunk = j & 127;
         const ulonglong2 t = *reinterpret_cast<const ulonglong2 *>(tile + rr * 256 + swz_chunk(chunk) * 2);
@@ -337,6 +339,11 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
         ulonglong2 o;
         o.x = shoup_canon(sub_mod(l.x, t.x, q), pinv.w, pinv.wq, q);
         o.y = shoup_canon(sub_mod(l.y, t.y, q), pinv.w, pinv.wq, q);
+        if (add) {
+          const ulonglong2 e = *reinterpret_cast<const ulonglong2 *>(add + rr * 256 + chunk * 2);
+          o.x = add_mod(o.x, e.x, q);
+          o.y = add_mod(o.y, e.y, q);
+        }
         *reinterpret_cast<ulonglong2 *>(out + rr * 256 + chunk * 2) = o;
       }
     }

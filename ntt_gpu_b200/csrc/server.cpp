@@ -1,0 +1,453 @@
+// Continuous-batching key-switch server (ntt_b200_server_*, include/ntt_b200.h).
+//
+// Requests (key switch, relinearization, rotation) arrive from any host thread
+// and reference device-resident ciphertexts and keys. One scheduler thread
+// forms waves and launches them through ntt_b200_keyswitch_requests:
+//  - a wave is the oldest pending request's shape class (context, level) plus
+//    every later pending request of that class, up to max_batch;
+//  - a wave launches as soon as a lane (a CUDA stream) is free and its
+//    workspace fits the HBM budget next to the waves already in flight, so
+//    requests that arrive while others run are admitted as lanes and memory
+//    free up, and waves on different lanes overlap on the device;
+//  - workspace comes from the device's stream-ordered pool and is returned in
+//    stream order after the wave;
+//  - a host callback at the end of each wave's stream work records completion,
+//    so latency is measured from submission to the GPU finishing the wave.
+// The reference serves one request per Session transaction (src/resident.cpp,
+// include/ntt/openfhe_hybrid_adapter.hpp:163-181) and has no server; the
+// admission budget follows its Limits/Reservation model (src/resident.cpp:10-28).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ntt_b200.h"
+
+namespace {
+
+double now_us() {
+  using namespace std::chrono;
+  return duration<double, std::micro>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Ticket {
+  ntt_b200_context ctx = nullptr;
+  ntt_b200_ks_request req{};
+  int status = NTT_B200_NOT_READY;
+  std::string error;
+  double t_submit = 0, t_launch = 0, t_done = 0;
+  uint32_t wave_size = 0;
+  int lane = -1;
+};
+
+struct Lane {
+  cudaStream_t stream = nullptr;
+  bool busy = false, finished = false;
+  std::vector<uint64_t> wave;
+  size_t bytes = 0;
+  double t_finished = 0;
+};
+
+}  // namespace
+
+struct ntt_b200_server_s {
+  ntt_b200_server_config cfg{};
+  std::mutex mu;
+  std::condition_variable cv_sched, cv_done;
+  std::deque<uint64_t> pending;
+  std::unordered_map<uint64_t, Ticket> tickets;
+  std::vector<Lane> lanes;
+  uint64_t next_id = 1;
+  size_t in_use = 0, peak_in_use = 0;
+  bool stopping = false;
+  std::string fatal;  // first CUDA failure; the server refuses new work after it
+  std::thread sched;
+  // statistics since the last reset
+  std::vector<double> latencies_us;
+  uint64_t waves = 0, wave_requests = 0;
+  double first_submit = 0, last_done = 0;
+
+  struct CallbackArg {
+    ntt_b200_server_s *srv;
+    int lane;
+  };
+  std::vector<CallbackArg> cb_args;
+
+  // Runs on the CUDA callback thread when a lane's wave finished on the GPU.
+  // It makes no CUDA calls.
+  static void CUDART_CB on_wave_done(void *p) {
+    auto *a = static_cast<CallbackArg *>(p);
+    const double t = now_us();
+    std::lock_guard<std::mutex> lock(a->srv->mu);
+    Lane &l = a->srv->lanes[a->lane];
+    l.finished = true;
+    l.t_finished = t;
+    a->srv->cv_sched.notify_all();
+  }
+
+  // Retire finished lanes (lock held).
+  void retire() {
+    for (Lane &l : lanes) {
+      if (!l.busy || !l.finished) continue;
+      for (uint64_t id : l.wave) {
+        auto it = tickets.find(id);
+        if (it == tickets.end()) continue;
+        Ticket &t = it->second;
+        t.status = NTT_B200_OK;
+        t.t_done = l.t_finished;
+        latencies_us.push_back(t.t_done - t.t_submit);
+        last_done = std::max(last_done, t.t_done);
+      }
+      in_use -= l.bytes;
+      l.busy = l.finished = false;
+      l.wave.clear();
+      l.bytes = 0;
+      cv_done.notify_all();
+    }
+  }
+
+  void fail_ticket(uint64_t id, int status, const std::string &why) {
+    auto it = tickets.find(id);
+    if (it == tickets.end()) return;
+    it->second.status = status;
+    it->second.error = why;
+    it->second.t_done = now_us();
+    cv_done.notify_all();
+  }
+
+  void erase_pending(const std::vector<uint64_t> &ids) {
+    for (uint64_t id : ids) {
+      auto it = std::find(pending.begin(), pending.end(), id);
+      if (it != pending.end()) pending.erase(it);
+    }
+  }
+
+  bool any_busy() const {
+    for (const Lane &l : lanes)
+      if (l.busy) return true;
+    return false;
+  }
+
+  // Form and launch at most one wave. Called with the lock held; the lock is
+  // released around the CUDA calls (the completion callback takes it too).
+  // Returns true if it made progress.
+  bool launch_one(std::unique_lock<std::mutex> &lock) {
+    if (pending.empty()) return false;
+    if (!fatal.empty()) {
+      for (uint64_t id : pending) fail_ticket(id, NTT_B200_ERR_CUDA, fatal);
+      pending.clear();
+      return false;
+    }
+    int lane = -1;
+    for (size_t i = 0; i < lanes.size(); ++i)
+      if (!lanes[i].busy) {
+        lane = (int)i;
+        break;
+      }
+    if (lane < 0) return false;
+    const Ticket &head = tickets[pending.front()];
+    const ntt_b200_context ctx = head.ctx;
+    const uint32_t level = head.req.level;
+    std::vector<uint64_t> wave;
+    std::vector<ntt_b200_ks_request> reqs;
+    for (uint64_t id : pending) {
+      if ((int)wave.size() >= cfg.max_batch) break;
+      const Ticket &t = tickets[id];
+      if (t.ctx != ctx || t.req.level != level) continue;
+      wave.push_back(id);
+      reqs.push_back(t.req);
+    }
+    // Shrink the wave until its workspace fits the budget left.
+    size_t need = 0;
+    while (true) {
+      if (ntt_b200_keyswitch_requests_workspace(ctx, reqs.data(), reqs.size(), &need) != NTT_B200_OK) {
+        // Requests are validated at submission; a failure here fails the wave.
+        const std::string why = ntt_b200_last_error();
+        for (uint64_t id : wave) fail_ticket(id, NTT_B200_ERR_CONTRACT, why);
+        erase_pending(wave);
+        return true;
+      }
+      if (in_use + need <= cfg.hbm_budget_bytes) break;
+      if (reqs.size() == 1) {
+        if (need > cfg.hbm_budget_bytes) {
+          fail_ticket(wave[0], NTT_B200_ERR_WORKSPACE, "request workspace exceeds the server's HBM budget");
+          erase_pending(wave);
+          return true;
+        }
+        return false;  // wait for in-flight waves to release memory
+      }
+      const size_t keep = reqs.size() / 2;
+      reqs.resize(keep);
+      wave.resize(keep);
+    }
+    // Reserve the lane and the memory, then launch without the lock.
+    erase_pending(wave);
+    const double t_launch = now_us();
+    for (uint64_t id : wave) {
+      Ticket &tk = tickets[id];
+      tk.t_launch = t_launch;
+      tk.wave_size = (uint32_t)wave.size();
+      tk.lane = lane;
+    }
+    {
+      Lane &l = lanes[lane];
+      l.busy = true;
+      l.finished = false;
+      l.wave = wave;
+      l.bytes = need;
+    }
+    in_use += need;
+    peak_in_use = std::max(peak_in_use, in_use);
+    const cudaStream_t stream = lanes[lane].stream;
+    lock.unlock();
+    int rc = NTT_B200_OK;
+    std::string why;
+    void *ws = nullptr;
+    cudaError_t e = cudaMallocAsync(&ws, std::max<size_t>(need, 256), stream);
+    if (e != cudaSuccess) {
+      rc = NTT_B200_ERR_CUDA;
+      why = std::string("CUDA: cudaMallocAsync: ") + cudaGetErrorString(e);
+    } else {
+      rc = ntt_b200_keyswitch_requests(ctx, reqs.data(), reqs.size(), ws, need, stream);
+      if (rc != NTT_B200_OK) why = ntt_b200_last_error();
+      cudaFreeAsync(ws, stream);
+      if (rc == NTT_B200_OK) {
+        e = cudaLaunchHostFunc(stream, &ntt_b200_server_s::on_wave_done, &cb_args[lane]);
+        if (e != cudaSuccess) {
+          rc = NTT_B200_ERR_CUDA;
+          why = std::string("CUDA: cudaLaunchHostFunc: ") + cudaGetErrorString(e);
+        }
+      }
+    }
+    lock.lock();
+    if (rc != NTT_B200_OK) {
+      Lane &l = lanes[lane];
+      l.busy = l.finished = false;
+      l.wave.clear();
+      l.bytes = 0;
+      in_use -= need;
+      for (uint64_t id : wave) fail_ticket(id, rc, why);
+      if (rc == NTT_B200_ERR_CUDA && fatal.empty()) fatal = why;
+      return true;
+    }
+    waves += 1;
+    wave_requests += wave.size();
+    return true;
+  }
+
+  void run() {
+    cudaSetDevice(cfg.device);
+    std::unique_lock<std::mutex> lock(mu);
+    while (true) {
+      retire();
+      while (launch_one(lock)) retire();
+      if (stopping && pending.empty() && !any_busy()) break;
+      cv_sched.wait(lock);
+    }
+  }
+};
+
+namespace {
+thread_local std::string g_server_error;
+
+template <class F> int server_guard(F f) {
+  try {
+    return f();
+  } catch (const std::exception &e) {
+    g_server_error = e.what();
+    return NTT_B200_ERR_CUDA;
+  }
+}
+
+int contract(const char *why) {
+  g_server_error = why;
+  return NTT_B200_ERR_CONTRACT;
+}
+
+double percentile(std::vector<double> v, double p) {
+  if (v.empty()) return 0;
+  std::sort(v.begin(), v.end());
+  const size_t i = (size_t)std::min<double>((double)v.size() - 1, p * (double)(v.size() - 1) + 0.5);
+  return v[i];
+}
+}  // namespace
+
+extern "C" {
+
+const char *ntt_b200_server_last_error(void) { return g_server_error.c_str(); }
+
+int ntt_b200_server_create(ntt_b200_server *out, const ntt_b200_server_config *cfg) {
+  return server_guard([&] {
+    if (!out || !cfg) return contract("null argument");
+    *out = nullptr;
+    if (cfg->device < 0 || cfg->lanes < 1 || cfg->lanes > 16 || cfg->max_batch < 1 || cfg->max_batch > 1024 ||
+        cfg->hbm_budget_bytes == 0)
+      return contract("invalid server configuration (1..16 lanes, 1..1024 batch, nonzero budget)");
+    auto *s = new ntt_b200_server_s();
+    s->cfg = *cfg;
+    cudaError_t e = cudaSetDevice(cfg->device);
+    s->lanes.resize(cfg->lanes);
+    s->cb_args.resize(cfg->lanes);
+    for (int i = 0; i < cfg->lanes && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&s->lanes[i].stream, cudaStreamNonBlocking);
+      s->cb_args[i] = {s, i};
+    }
+    if (e == cudaSuccess) {
+      cudaMemPool_t pool;
+      e = cudaDeviceGetDefaultMemPool(&pool, cfg->device);
+      uint64_t keep = UINT64_MAX;  // keep freed workspace cached for the next wave
+      if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (e != cudaSuccess) {
+      for (Lane &l : s->lanes)
+        if (l.stream) cudaStreamDestroy(l.stream);
+      delete s;
+      g_server_error = std::string("CUDA: server streams: ") + cudaGetErrorString(e);
+      return NTT_B200_ERR_CUDA;
+    }
+    s->sched = std::thread([s] { s->run(); });
+    *out = s;
+    return NTT_B200_OK;
+  });
+}
+
+int ntt_b200_server_submit(ntt_b200_server srv, ntt_b200_context ctx, const ntt_b200_ks_request *req,
+                           uint64_t *ticket) {
+  return server_guard([&] {
+    if (!srv || !ctx || !req || !ticket) return contract("null argument");
+    // Validate the request alone before it joins a wave: a bad request is
+    // refused here and never fails the requests it would have been batched with.
+    size_t need = 0;
+    if (ntt_b200_keyswitch_requests_workspace(ctx, req, 1, &need) != NTT_B200_OK) {
+      g_server_error = ntt_b200_last_error();
+      return NTT_B200_ERR_CONTRACT;
+    }
+    std::lock_guard<std::mutex> lock(srv->mu);
+    if (srv->stopping) return contract("server is shutting down");
+    if (!srv->fatal.empty()) {
+      g_server_error = srv->fatal;
+      return NTT_B200_ERR_CUDA;
+    }
+    if (need > srv->cfg.hbm_budget_bytes) {
+      g_server_error = "request workspace exceeds the server's HBM budget";
+      return NTT_B200_ERR_WORKSPACE;
+    }
+    const uint64_t id = srv->next_id++;
+    Ticket t;
+    t.ctx = ctx;
+    t.req = *req;
+    t.t_submit = now_us();
+    if (srv->first_submit == 0) srv->first_submit = t.t_submit;
+    srv->tickets.emplace(id, std::move(t));
+    srv->pending.push_back(id);
+    *ticket = id;
+    srv->cv_sched.notify_all();
+    return NTT_B200_OK;
+  });
+}
+
+int ntt_b200_server_wait(ntt_b200_server srv, uint64_t ticket, uint32_t timeout_ms, ntt_b200_ticket_info *info) {
+  return server_guard([&] {
+    if (!srv) return contract("null server");
+    std::unique_lock<std::mutex> lock(srv->mu);
+    auto it = srv->tickets.find(ticket);
+    if (it == srv->tickets.end()) return contract("unknown or already collected ticket");
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+    while (it->second.status == NTT_B200_NOT_READY) {
+      if (srv->cv_done.wait_until(lock, deadline) == std::cv_status::timeout &&
+          srv->tickets.find(ticket)->second.status == NTT_B200_NOT_READY) {
+        g_server_error = "ticket not complete within the timeout";
+        return NTT_B200_ERR_TIMEOUT;
+      }
+      it = srv->tickets.find(ticket);
+    }
+    const Ticket &t = it->second;
+    if (info) {
+      info->status = t.status;
+      info->wave_size = t.wave_size;
+      info->lane = t.lane;
+      info->queue_us = t.t_launch > 0 ? t.t_launch - t.t_submit : 0;
+      info->latency_us = t.t_done - t.t_submit;
+    }
+    const int status = t.status;
+    if (status != NTT_B200_OK) g_server_error = t.error;
+    srv->tickets.erase(it);
+    return status;
+  });
+}
+
+int ntt_b200_server_drain(ntt_b200_server srv, uint32_t timeout_ms) {
+  return server_guard([&] {
+    if (!srv) return contract("null server");
+    std::unique_lock<std::mutex> lock(srv->mu);
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+    while (!srv->pending.empty() || srv->any_busy()) {
+      if (srv->cv_done.wait_until(lock, deadline) == std::cv_status::timeout &&
+          (!srv->pending.empty() || srv->any_busy())) {
+        g_server_error = "server did not drain within the timeout";
+        return NTT_B200_ERR_TIMEOUT;
+      }
+    }
+    if (!srv->fatal.empty()) {
+      g_server_error = srv->fatal;
+      return NTT_B200_ERR_CUDA;
+    }
+    return NTT_B200_OK;
+  });
+}
+
+int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int reset) {
+  return server_guard([&] {
+    if (!srv || !out) return contract("null argument");
+    std::lock_guard<std::mutex> lock(srv->mu);
+    std::memset(out, 0, sizeof(*out));
+    out->completed = srv->latencies_us.size();
+    out->waves = srv->waves;
+    out->mean_wave = srv->waves ? (double)srv->wave_requests / (double)srv->waves : 0;
+    out->p50_ms = percentile(srv->latencies_us, 0.50) / 1000.0;
+    out->p99_ms = percentile(srv->latencies_us, 0.99) / 1000.0;
+    out->max_ms = srv->latencies_us.empty()
+                      ? 0
+                      : *std::max_element(srv->latencies_us.begin(), srv->latencies_us.end()) / 1000.0;
+    const double span = srv->last_done - srv->first_submit;
+    out->throughput = span > 0 ? (double)out->completed / (span / 1e6) : 0;
+    out->peak_bytes = srv->peak_in_use;
+    out->in_flight_bytes = srv->in_use;
+    if (reset) {
+      srv->latencies_us.clear();
+      srv->waves = srv->wave_requests = 0;
+      srv->first_submit = srv->last_done = 0;
+      srv->peak_in_use = srv->in_use;
+    }
+    return NTT_B200_OK;
+  });
+}
+
+int ntt_b200_server_destroy(ntt_b200_server srv) {
+  return server_guard([&] {
+    if (!srv) return NTT_B200_OK;
+    {
+      std::lock_guard<std::mutex> lock(srv->mu);
+      srv->stopping = true;
+      srv->cv_sched.notify_all();
+    }
+    srv->sched.join();  // drains pending work first
+    for (Lane &l : srv->lanes) {
+      cudaStreamSynchronize(l.stream);
+      cudaStreamDestroy(l.stream);
+    }
+    delete srv;
+    return NTT_B200_OK;
+  });
+}
+
+}  // extern "C"
