@@ -297,7 +297,8 @@ def serve_poisson(nb, srv, jobs, rate, seed):
     waves = [srv.wait(t).wave_size for t in tickets]
     st = srv.stats(reset=True)
     return {"offered_per_s": rate, "throughput": st["throughput"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "max_ms": st["max_ms"], "mean_wave": sum(waves) / len(waves), "requests": len(jobs)}
+            "max_ms": st["max_ms"], "mean_queue_ms": st["mean_queue_ms"], "mean_wave": sum(waves) / len(waves),
+            "requests": len(jobs)}
 
 
 def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
@@ -306,8 +307,12 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
 
     from ntt_gpu_b200.params import synthetic_params
     budget = 40 << 30
-    out = {"served_server": {"lanes": 2, "max_batch": BATCH, "hbm_budget_bytes": budget},
-           "plain_server": {"lanes": 1, "max_batch": 1, "hbm_budget_bytes": budget},
+    served_cfg = {"lanes": 2, "max_batch": BATCH, "depth": 1, "hbm_budget_bytes": budget}
+    plain_cfg = {"lanes": 1, "max_batch": 1, "depth": 2, "hbm_budget_bytes": budget}
+    legs = (("served", served_cfg), ("plain", plain_cfg))
+    out = {"served_server": served_cfg,
+           "plain_server": dict(plain_cfg, note="same kernels, one request per wave, the next request queued "
+                                                "behind the running one on one stream"),
            "arrivals": f"seeded Poisson (numpy default_rng, seed {seed:#x})"}
     # (1) the headline shape: N=2^16, L=24, dnum=3, K=8, key switches.
     prm = synthetic_params(N, LEVEL, K_P, DNUM)
@@ -316,8 +321,8 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
     rates = sorted({round(plain_value * f) for f in (0.5, 0.9, 1.3)} | {round(batched_value * 0.9)})
     for rate in rates:
         row = {}
-        for name, lanes, mb in (("served", 2, BATCH), ("plain", 1, 1)):
-            srv = nb.Server(device=device, lanes=lanes, max_batch=mb, hbm_budget_bytes=budget)
+        for name, cfg in legs:
+            srv = nb.Server(device=device, **cfg)
             count = max(64, min(400, int(rate * 0.12)))
             jobs = [(w.ctx, w.request(nb, LEVEL, "switch", 0, i)) for i in range(count)]
             serve_poisson(nb, srv, jobs[:16], rate, seed + 1)  # warm-up
@@ -350,7 +355,7 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
             jobs.append((wk.ctx, wk.request(nb, level, kind, step, i)))
         return jobs
 
-    srv = nb.Server(device=device, lanes=2, max_batch=BATCH, hbm_budget_bytes=budget)
+    srv = nb.Server(device=device, **served_cfg)
     burst = mixed_jobs(600, seed + 3)
     serve_poisson(nb, srv, burst[:40], 1e6, seed + 4)
     cap = serve_poisson(nb, srv, burst, 1e7, seed + 5)["throughput"]  # saturation: all arrive at once
@@ -359,8 +364,8 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
     for frac in (0.5, 0.9):
         rate = cap * frac
         row = {}
-        for name, lanes, mb in (("served", 2, BATCH), ("plain", 1, 1)):
-            srv = nb.Server(device=device, lanes=lanes, max_batch=mb, hbm_budget_bytes=budget)
+        for name, cfg in legs:
+            srv = nb.Server(device=device, **cfg)
             jobs = mixed_jobs(max(100, min(600, int(rate * 0.25))), seed + 7)
             row[name] = serve_poisson(nb, srv, jobs, rate, seed + 8)
             srv.close()

@@ -201,8 +201,8 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
  * device-resident ciphertexts and keys that the caller keeps alive until the
  * ticket completes. A scheduler thread forms waves of the oldest pending
  * request's (context, level) class, up to max_batch, and launches each on the
- * first free lane (a CUDA stream) once its workspace fits hbm_budget_bytes next
- * to the waves in flight: requests arriving while others run join the next
+ * least-loaded lane (a CUDA stream with fewer than `depth` waves in flight)
+ * once its workspace fits hbm_budget_bytes next to the waves in flight: requests arriving while others run join the next
  * wave as lanes and memory free up, and waves on different lanes overlap on
  * the device. Each result equals the request run alone. The reference has no
  * server (one request per Session transaction, src/resident.cpp); admission
@@ -210,9 +210,9 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
 typedef struct ntt_b200_server_s *ntt_b200_server;
 typedef struct ntt_b200_server_config {
   int device;
-  int lanes;      /* concurrent waves (CUDA streams), 1..16 */
+  int lanes;      /* CUDA streams that run waves concurrently, 1..16 */
   int max_batch;  /* requests per wave, 1..1024 */
-  int reserved;
+  int depth;      /* waves in flight per lane, 1..8 (0 = 1); >1 queues the next wave behind the running one */
   size_t hbm_budget_bytes; /* workspace of all in-flight waves */
 } ntt_b200_server_config;
 typedef struct ntt_b200_ticket_info {
@@ -227,6 +227,7 @@ typedef struct ntt_b200_server_report {
   uint64_t completed, waves;
   double mean_wave, p50_ms, p99_ms, max_ms;
   double throughput;   /* completed / (last completion - first submission), per second */
+  double mean_queue_ms; /* submission -> wave launch, mean */
   size_t peak_bytes, in_flight_bytes;
 } ntt_b200_server_report;
 const char *ntt_b200_server_last_error(void);

@@ -99,7 +99,7 @@ class KsRequest(ctypes.Structure):
 
 
 class ServerConfig(ctypes.Structure):
-    _fields_ = [("device", _I), ("lanes", _I), ("max_batch", _I), ("reserved", _I), ("hbm_budget_bytes", _SZ)]
+    _fields_ = [("device", _I), ("lanes", _I), ("max_batch", _I), ("depth", _I), ("hbm_budget_bytes", _SZ)]
 
 
 class TicketInfo(ctypes.Structure):
@@ -110,7 +110,7 @@ class TicketInfo(ctypes.Structure):
 class ServerReport(ctypes.Structure):
     _fields_ = [("completed", _U64), ("waves", _U64), ("mean_wave", ctypes.c_double), ("p50_ms", ctypes.c_double),
                 ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("throughput", ctypes.c_double),
-                ("peak_bytes", _SZ), ("in_flight_bytes", _SZ)]
+                ("mean_queue_ms", ctypes.c_double), ("peak_bytes", _SZ), ("in_flight_bytes", _SZ)]
 
 
 def make_request(level, src, out_b, out_a, key_b, key_a, c0=None, automorphism=0, add_b=None, add_a=None):
@@ -312,9 +312,9 @@ class Server:
     request's wave finished on the GPU and returns its TicketInfo.
     """
 
-    def __init__(self, device=0, lanes=2, max_batch=16, hbm_budget_bytes=8 << 30):
+    def __init__(self, device=0, lanes=2, max_batch=16, hbm_budget_bytes=8 << 30, depth=1):
         self._lib = load()
-        cfg = ServerConfig(int(device), int(lanes), int(max_batch), 0, int(hbm_budget_bytes))
+        cfg = ServerConfig(int(device), int(lanes), int(max_batch), int(depth), int(hbm_budget_bytes))
         h = _P()
         _check(self._lib.ntt_b200_server_create(ctypes.byref(h), ctypes.byref(cfg)), server=True)
         self._h = h

@@ -5,10 +5,11 @@
 // forms waves and launches them through ntt_b200_keyswitch_requests:
 //  - a wave is the oldest pending request's shape class (context, level) plus
 //    every later pending request of that class, up to max_batch;
-//  - a wave launches as soon as a lane (a CUDA stream) is free and its
-//    workspace fits the HBM budget next to the waves already in flight, so
-//    requests that arrive while others run are admitted as lanes and memory
-//    free up, and waves on different lanes overlap on the device;
+//  - a wave launches as soon as a lane (a CUDA stream) has fewer than `depth`
+//    waves in flight and its workspace fits the HBM budget next to the waves
+//    already in flight, so requests that arrive while others run are admitted
+//    as lanes and memory free up, and waves on different lanes overlap on the
+//    device (a depth above 1 queues the next wave behind the running one);
 //  - workspace comes from the device's stream-ordered pool and is returned in
 //    stream order after the wave;
 //  - a host callback at the end of each wave's stream work records completion,
@@ -24,6 +25,7 @@
 #include <cstdint>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -49,12 +51,19 @@ struct Ticket {
   int lane = -1;
 };
 
+// One launched wave; its address is the completion callback's argument.
+struct Wave {
+  ntt_b200_server_s *srv = nullptr;
+  int lane = -1;
+  std::vector<uint64_t> ids;
+  size_t bytes = 0;
+  bool finished = false;
+  double t_finished = 0;
+};
+
 struct Lane {
   cudaStream_t stream = nullptr;
-  bool busy = false, finished = false;
-  std::vector<uint64_t> wave;
-  size_t bytes = 0;
-  double t_finished = 0;
+  int inflight = 0;  // waves enqueued on this stream and not yet retired
 };
 
 }  // namespace
@@ -66,6 +75,8 @@ struct ntt_b200_server_s {
   std::deque<uint64_t> pending;
   std::unordered_map<uint64_t, Ticket> tickets;
   std::vector<Lane> lanes;
+  std::unordered_map<Wave *, std::unique_ptr<Wave>> waves_in_flight;
+  int depth = 1;
   uint64_t next_id = 1;
   size_t in_use = 0, peak_in_use = 0;
   bool stopping = false;
@@ -74,43 +85,39 @@ struct ntt_b200_server_s {
   // statistics since the last reset
   std::vector<double> latencies_us;
   uint64_t waves = 0, wave_requests = 0;
-  double first_submit = 0, last_done = 0;
+  double first_submit = 0, last_done = 0, queue_us = 0;
 
-  struct CallbackArg {
-    ntt_b200_server_s *srv;
-    int lane;
-  };
-  std::vector<CallbackArg> cb_args;
-
-  // Runs on the CUDA callback thread when a lane's wave finished on the GPU.
-  // It makes no CUDA calls.
+  // Runs on the CUDA callback thread when a wave finished on the GPU. It
+  // makes no CUDA calls.
   static void CUDART_CB on_wave_done(void *p) {
-    auto *a = static_cast<CallbackArg *>(p);
+    auto *w = static_cast<Wave *>(p);
     const double t = now_us();
-    std::lock_guard<std::mutex> lock(a->srv->mu);
-    Lane &l = a->srv->lanes[a->lane];
-    l.finished = true;
-    l.t_finished = t;
-    a->srv->cv_sched.notify_all();
+    std::lock_guard<std::mutex> lock(w->srv->mu);
+    w->finished = true;
+    w->t_finished = t;
+    w->srv->cv_sched.notify_all();
   }
 
-  // Retire finished lanes (lock held).
+  // Retire finished waves (lock held).
   void retire() {
-    for (Lane &l : lanes) {
-      if (!l.busy || !l.finished) continue;
-      for (uint64_t id : l.wave) {
-        auto it = tickets.find(id);
-        if (it == tickets.end()) continue;
-        Ticket &t = it->second;
-        t.status = NTT_B200_OK;
-        t.t_done = l.t_finished;
-        latencies_us.push_back(t.t_done - t.t_submit);
-        last_done = std::max(last_done, t.t_done);
+    for (auto it = waves_in_flight.begin(); it != waves_in_flight.end();) {
+      Wave &w = *it->second;
+      if (!w.finished) {
+        ++it;
+        continue;
       }
-      in_use -= l.bytes;
-      l.busy = l.finished = false;
-      l.wave.clear();
-      l.bytes = 0;
+      for (uint64_t id : w.ids) {
+        auto t = tickets.find(id);
+        if (t == tickets.end()) continue;
+        t->second.status = NTT_B200_OK;
+        t->second.t_done = w.t_finished;
+        latencies_us.push_back(w.t_finished - t->second.t_submit);
+        queue_us += t->second.t_launch - t->second.t_submit;
+        last_done = std::max(last_done, w.t_finished);
+      }
+      in_use -= w.bytes;
+      lanes[w.lane].inflight -= 1;
+      it = waves_in_flight.erase(it);
       cv_done.notify_all();
     }
   }
@@ -131,11 +138,7 @@ struct ntt_b200_server_s {
     }
   }
 
-  bool any_busy() const {
-    for (const Lane &l : lanes)
-      if (l.busy) return true;
-    return false;
-  }
+  bool any_busy() const { return !waves_in_flight.empty(); }
 
   // Form and launch at most one wave. Called with the lock held; the lock is
   // released around the CUDA calls (the completion callback takes it too).
@@ -147,12 +150,9 @@ struct ntt_b200_server_s {
       pending.clear();
       return false;
     }
-    int lane = -1;
+    int lane = -1;  // the lane with the fewest waves in flight, below the depth
     for (size_t i = 0; i < lanes.size(); ++i)
-      if (!lanes[i].busy) {
-        lane = (int)i;
-        break;
-      }
+      if (lanes[i].inflight < depth && (lane < 0 || lanes[i].inflight < lanes[lane].inflight)) lane = (int)i;
     if (lane < 0) return false;
     const Ticket &head = tickets[pending.front()];
     const ntt_b200_context ctx = head.ctx;
@@ -198,13 +198,13 @@ struct ntt_b200_server_s {
       tk.wave_size = (uint32_t)wave.size();
       tk.lane = lane;
     }
-    {
-      Lane &l = lanes[lane];
-      l.busy = true;
-      l.finished = false;
-      l.wave = wave;
-      l.bytes = need;
-    }
+    auto owned = std::make_unique<Wave>();
+    Wave *wv = owned.get();
+    wv->srv = this;
+    wv->lane = lane;
+    wv->ids = wave;
+    wv->bytes = need;
+    lanes[lane].inflight += 1;
     in_use += need;
     peak_in_use = std::max(peak_in_use, in_use);
     const cudaStream_t stream = lanes[lane].stream;
@@ -221,7 +221,7 @@ struct ntt_b200_server_s {
       if (rc != NTT_B200_OK) why = ntt_b200_last_error();
       cudaFreeAsync(ws, stream);
       if (rc == NTT_B200_OK) {
-        e = cudaLaunchHostFunc(stream, &ntt_b200_server_s::on_wave_done, &cb_args[lane]);
+        e = cudaLaunchHostFunc(stream, &ntt_b200_server_s::on_wave_done, wv);
         if (e != cudaSuccess) {
           rc = NTT_B200_ERR_CUDA;
           why = std::string("CUDA: cudaLaunchHostFunc: ") + cudaGetErrorString(e);
@@ -230,15 +230,13 @@ struct ntt_b200_server_s {
     }
     lock.lock();
     if (rc != NTT_B200_OK) {
-      Lane &l = lanes[lane];
-      l.busy = l.finished = false;
-      l.wave.clear();
-      l.bytes = 0;
+      lanes[lane].inflight -= 1;
       in_use -= need;
       for (uint64_t id : wave) fail_ticket(id, rc, why);
       if (rc == NTT_B200_ERR_CUDA && fatal.empty()) fatal = why;
       return true;
     }
+    waves_in_flight.emplace(wv, std::move(owned));
     waves += 1;
     wave_requests += wave.size();
     return true;
@@ -292,15 +290,14 @@ int ntt_b200_server_create(ntt_b200_server *out, const ntt_b200_server_config *c
     if (cfg->device < 0 || cfg->lanes < 1 || cfg->lanes > 16 || cfg->max_batch < 1 || cfg->max_batch > 1024 ||
         cfg->hbm_budget_bytes == 0)
       return contract("invalid server configuration (1..16 lanes, 1..1024 batch, nonzero budget)");
+    if (cfg->depth < 0 || cfg->depth > 8) return contract("invalid server configuration (depth 0..8)");
     auto *s = new ntt_b200_server_s();
     s->cfg = *cfg;
+    s->depth = cfg->depth ? cfg->depth : 1;
     cudaError_t e = cudaSetDevice(cfg->device);
     s->lanes.resize(cfg->lanes);
-    s->cb_args.resize(cfg->lanes);
-    for (int i = 0; i < cfg->lanes && e == cudaSuccess; ++i) {
+    for (int i = 0; i < cfg->lanes && e == cudaSuccess; ++i)
       e = cudaStreamCreateWithFlags(&s->lanes[i].stream, cudaStreamNonBlocking);
-      s->cb_args[i] = {s, i};
-    }
     if (e == cudaSuccess) {
       cudaMemPool_t pool;
       e = cudaDeviceGetDefaultMemPool(&pool, cfg->device);
@@ -420,12 +417,13 @@ int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int 
                       : *std::max_element(srv->latencies_us.begin(), srv->latencies_us.end()) / 1000.0;
     const double span = srv->last_done - srv->first_submit;
     out->throughput = span > 0 ? (double)out->completed / (span / 1e6) : 0;
+    out->mean_queue_ms = out->completed ? srv->queue_us / (double)out->completed / 1000.0 : 0;
     out->peak_bytes = srv->peak_in_use;
     out->in_flight_bytes = srv->in_use;
     if (reset) {
       srv->latencies_us.clear();
       srv->waves = srv->wave_requests = 0;
-      srv->first_submit = srv->last_done = 0;
+      srv->first_submit = srv->last_done = srv->queue_us = 0;
       srv->peak_in_use = srv->in_use;
     }
     return NTT_B200_OK;

@@ -48,10 +48,11 @@ def _check(orc, cases):
         np.testing.assert_array_equal(nb.to_host(c.out_a), wa, err_msg=f"{c.kind} N={ctx.n} L={c.level}")
 
 
-def test_served_results_equal_oracle_under_concurrent_arrivals(lib, orc):
+@pytest.mark.parametrize("lanes,depth,max_batch", [(3, 1, 8), (1, 2, 1), (2, 3, 4)])
+def test_served_results_equal_oracle_under_concurrent_arrivals(lib, orc, lanes, depth, max_batch):
     contexts = _contexts(orc)
-    cases = _random_cases(orc, contexts, 48, 7)
-    srv = nb.Server(device=0, lanes=3, max_batch=8, hbm_budget_bytes=2 << 30)
+    cases = _random_cases(orc, contexts, 48, 7 + lanes)
+    srv = nb.Server(device=0, lanes=lanes, max_batch=max_batch, hbm_budget_bytes=2 << 30, depth=depth)
     tickets = {}
 
     def producer(part, delay_s):
