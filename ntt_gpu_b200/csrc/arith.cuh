@@ -2,9 +2,10 @@
 //
 // Residues are u64 and every public result is canonical ([0, q)), matching the
 // reference contract (docs/modular-arithmetic-contract.md:25-31 in
-// minnow54426/ntt-gpu). Internally the NTT uses Harvey's lazy butterflies:
-// values live in [0, 4q) between stages, which needs q < 2^62 ("lazy" moduli);
-// moduli in [2^62, 2^63) take the strict path where every value stays canonical.
+// minnow54426/ntt-gpu). Internally the NTT keeps lazy ranges between stages
+// (the butterfly MODEs below): moduli below 2^61 take the fast path, moduli
+// below 2^62 Harvey's lazy butterflies, and moduli in [2^62, 2^63) the strict
+// path where every value stays canonical.
 //
 // Multiplication by a constant w uses Shoup's precomputed quotient
 // w' = floor(w * 2^64 / q) (reference include/ntt/shoup.hpp:7-27): for ANY
@@ -33,11 +34,48 @@ __device__ __forceinline__ u64 add_mod(u64 a, u64 b, u64 q) { return csub(a + b,
 __device__ __forceinline__ u64 sub_mod(u64 a, u64 b, u64 q) { return a >= b ? a - b : a + (q - b); }
 
 // ---- NTT butterflies --------------------------------------------------------
+// MODE selects the value ranges kept between stages:
+//   0 strict: canonical in and out (any q < 2^63);
+//   1 lazy:   Harvey's butterflies, forward [0, 4q), inverse [0, 2q) (q < 2^62);
+//   2 fast:   approximate-quotient Shoup products (below), forward [0, 8q),
+//             inverse [0, 4q) (q < 2^61).
+
+// Shoup product with an approximate quotient, for any x < 2^64 and q < 2^62.
+// With x = xh:xl and w' = wh:wl (32-bit halves), the quotient estimate is
+// xh*wh + hi(xl*wh) + hi(xh*wl): it drops xl*wl and every carry between the
+// partial products, so it is at most 2 below floor(x*w'/2^64), which is itself
+// at most 1 below floor(x*w/q). Hence x*w - estimate*q lies in [0, 4q); it is
+// formed mod 2^64 as x*w + estimate*(2^64 - q). Every product is a multiply-add,
+// none of them needs a carry fix-up, and no comparison is involved.
+__device__ __forceinline__ u64 shoup_approx(u64 x, u64 w, u64 wq, u64 qneg) {
+  const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32);
+  const uint32_t wl = (uint32_t)wq, wh = (uint32_t)(wq >> 32);
+  uint32_t h1, h2;
+  u64 qh, r;
+  asm("mul.hi.u32 %0, %1, %2;" : "=r"(h1) : "r"(xl), "r"(wh));
+  asm("mul.hi.u32 %0, %1, %2;" : "=r"(h2) : "r"(xh), "r"(wl));
+  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(qh) : "r"(xh), "r"(wh), "l"((u64)h1));
+  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(qh) : "r"(h2), "r"(1u), "l"(qh));
+  asm("mul.lo.u64 %0, %1, %2;" : "=l"(r) : "l"(x), "l"(w));
+  asm("mad.lo.u64 %0, %1, %2, %3;" : "=l"(r) : "l"(qh), "l"(qneg), "l"(r));
+  return r;
+}
+// x - m if x >= m, else x; requires x - m in (-2^63, 2^63) (the sign decides).
+__device__ __forceinline__ u64 csub_sign(u64 x, u64 m) {
+  const u64 d = x - m;
+  return (int64_t)d < 0 ? x : d;
+}
+
 // Forward Cooley-Tukey (x, y) -> (x + w*y, x - w*y).
-// LAZY: inputs and outputs in [0, 4q). Strict: canonical in and out.
-template <bool LAZY>
+template <int MODE>
 __device__ __forceinline__ void ct_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 q, u64 q2) {
-  if constexpr (LAZY) {
+  if constexpr (MODE == 2) {
+    const u64 q4 = 2 * q2;
+    const u64 a = csub_sign(x, q4);  // [0, 8q) -> [0, 4q)
+    const u64 t = shoup_approx(y, w, wq, 0 - q);
+    x = a + t;
+    y = a + q4 - t;
+  } else if constexpr (MODE == 1) {
     const u64 a = csub(x, q2);
     const u64 t = shoup_lazy(y, w, wq, q);
     x = a + t;
@@ -51,10 +89,15 @@ __device__ __forceinline__ void ct_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 
 }
 
 // Inverse Gentleman-Sande (x, y) -> (x + y, (x - y) * w).
-// LAZY: inputs and outputs in [0, 2q). Strict: canonical.
-template <bool LAZY>
+template <int MODE>
 __device__ __forceinline__ void gs_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 q, u64 q2) {
-  if constexpr (LAZY) {
+  if constexpr (MODE == 2) {
+    const u64 q4 = 2 * q2;
+    const u64 s = csub_sign(x + y, q4);
+    const u64 d = x + q4 - y;
+    y = shoup_approx(d, w, wq, 0 - q);
+    x = s;
+  } else if constexpr (MODE == 1) {
     const u64 s = csub(x + y, q2);
     const u64 d = x + q2 - y;
     y = shoup_lazy(d, w, wq, q);
@@ -69,11 +112,12 @@ __device__ __forceinline__ void gs_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 
 
 // Last inverse stage with the N^-1 scale folded in: outputs canonical.
 // (x, y) -> ((x + y) * n_inv, (x - y) * w * n_inv); wn = w * n_inv.
-template <bool LAZY>
+template <int MODE>
 __device__ __forceinline__ void gs_last(u64 &x, u64 &y, Shoup ninv, Shoup wn, u64 q, u64 q2) {
-  if constexpr (LAZY) {
-    const u64 s = x + y;       // < 4q
-    const u64 d = x + q2 - y;  // < 4q
+  if constexpr (MODE != 0) {
+    const u64 span = MODE == 2 ? 2 * q2 : q2;  // inputs in [0, span)
+    const u64 s = x + y;
+    const u64 d = x + span - y;
     x = shoup_canon(s, ninv.w, ninv.wq, q);
     y = shoup_canon(d, wn.w, wn.wq, q);
   } else {
@@ -86,6 +130,13 @@ __device__ __forceinline__ void gs_last(u64 &x, u64 &y, Shoup ninv, Shoup wn, u6
 
 // [0, 4q) -> [0, q).
 __device__ __forceinline__ u64 reduce4(u64 x, u64 q, u64 q2) { return csub(csub(x, q2), q); }
+// A forward transform's stage range -> canonical.
+template <int MODE>
+__device__ __forceinline__ u64 reduce_final(u64 x, u64 q, u64 q2) {
+  if constexpr (MODE == 2) return csub_sign(csub_sign(csub_sign(x, 2 * q2), q2), q);
+  else if constexpr (MODE == 1) return reduce4(x, q, q2);
+  else return x;
+}
 
 // ---- 128-bit accumulation ------------------------------------------------------
 // Exact sums of u64 products for the approximate-CRT basis switch and the Hybrid

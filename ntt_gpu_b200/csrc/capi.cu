@@ -146,7 +146,7 @@ struct ntt_b200_context_s {
   u64 n = 0;
   int logn = 0;
   size_t m = 0, k = 0, alpha = 0;
-  bool lazy = true;
+  int mode = 2;  // NTT butterfly mode: 2 all moduli < 2^61, 1 all < 2^62, 0 otherwise
   std::vector<u64> mod, psi;  // [M + K] by global id
   b200::TowerConsts *d_tc = nullptr;
   ulonglong2 *d_fwd = nullptr, *d_inv = nullptr;
@@ -360,24 +360,24 @@ bool persistent_enabled() {
   return on;
 }
 
-template <int LOGN, bool LAZY, bool INV>
+template <int LOGN, int MODE, bool INV>
 void launch_col_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
   static int cache[64] = {0};
   constexpr int smem = b200::col_smem_bytes<LOGN>();
   const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
-  const unsigned grid = persistent_grid(b200::ntt_col_ps<LOGN, LAZY, INV>, smem, total, c.device, cache);
-  b200::ntt_col_ps<LOGN, LAZY, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
+  const unsigned grid = persistent_grid(b200::ntt_col_ps<LOGN, MODE, INV>, smem, total, c.device, cache);
+  b200::ntt_col_ps<LOGN, MODE, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
 }
-template <int LOGN, bool LAZY, bool INV>
+template <int LOGN, int MODE, bool INV>
 void launch_row_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
   static int cache[64] = {0};
   constexpr int smem = b200::kRowPsSmem;
   const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
-  const unsigned grid = persistent_grid(b200::ntt_row_ps<LOGN, LAZY, INV>, smem, total, c.device, cache);
-  b200::ntt_row_ps<LOGN, LAZY, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
+  const unsigned grid = persistent_grid(b200::ntt_row_ps<LOGN, MODE, INV>, smem, total, c.device, cache);
+  b200::ntt_row_ps<LOGN, MODE, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
 }
 
-template <int LOGN, bool LAZY>
+template <int LOGN, int MODE>
 void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
                       bool inverse, cudaStream_t st) {
   const dim3 grid((1u << LOGN) / b200::kTileWords, slots, polys);
@@ -399,47 +399,47 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     const uint32_t ns = (uint32_t)slots, np = (uint32_t)polys;
     if (!inverse) {
       Timed t1("ntt_fwd_col", st);
-      launch_col_ps<LOGN, LAZY, false>(c, b, ns, np, st);
+      launch_col_ps<LOGN, MODE, false>(c, b, ns, np, st);
       t1.done();
       Timed t2("ntt_fwd_row", st);
-      launch_row_ps<LOGN, LAZY, false>(c, second, ns, np, st);
+      launch_row_ps<LOGN, MODE, false>(c, second, ns, np, st);
       t2.done();
     } else {
       Timed t1("ntt_inv_row", st);
-      launch_row_ps<LOGN, LAZY, true>(c, b, ns, np, st);
+      launch_row_ps<LOGN, MODE, true>(c, b, ns, np, st);
       t1.done();
       Timed t2("ntt_inv_col", st);
-      launch_col_ps<LOGN, LAZY, true>(c, second, ns, np, st);
+      launch_col_ps<LOGN, MODE, true>(c, second, ns, np, st);
       t2.done();
     }
     return;
   }
   if (!inverse) {
     Timed t1("ntt_fwd_col", st);
-    b200::ntt_fwd_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
+    b200::ntt_fwd_col<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
     t1.done();
     Timed t2("ntt_fwd_row", st);
-    b200::ntt_fwd_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+    b200::ntt_fwd_row<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
     t2.done();
   } else {
     Timed t1("ntt_inv_row", st);
-    b200::ntt_inv_row<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
+    b200::ntt_inv_row<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
     t1.done();
     Timed t2("ntt_inv_col", st);
-    b200::ntt_inv_col<LOGN, LAZY><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+    b200::ntt_inv_col<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
     t2.done();
   }
 }
 
-template <bool LAZY>
+template <int MODE>
 void launch_ntt_chunk(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
                       bool inverse, cudaStream_t st) {
   switch (c.logn) {
-    case 12: launch_ntt_2pass<12, LAZY>(c, b, fin, slots, polys, inverse, st); break;
-    case 13: launch_ntt_2pass<13, LAZY>(c, b, fin, slots, polys, inverse, st); break;
-    case 14: launch_ntt_2pass<14, LAZY>(c, b, fin, slots, polys, inverse, st); break;
-    case 15: launch_ntt_2pass<15, LAZY>(c, b, fin, slots, polys, inverse, st); break;
-    case 16: launch_ntt_2pass<16, LAZY>(c, b, fin, slots, polys, inverse, st); break;
+    case 12: launch_ntt_2pass<12, MODE>(c, b, fin, slots, polys, inverse, st); break;
+    case 13: launch_ntt_2pass<13, MODE>(c, b, fin, slots, polys, inverse, st); break;
+    case 14: launch_ntt_2pass<14, MODE>(c, b, fin, slots, polys, inverse, st); break;
+    case 15: launch_ntt_2pass<15, MODE>(c, b, fin, slots, polys, inverse, st); break;
+    case 16: launch_ntt_2pass<16, MODE>(c, b, fin, slots, polys, inverse, st); break;
     default: throw ContractError("unsupported ring dimension");
   }
 }
@@ -502,10 +502,12 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
         b200::correct_kernel<<<ew_grid(c, count, polys), b200::kEwThreads, 0, st>>>(a);
         t.done();
       }
-    } else if (c.lazy) {
-      launch_ntt_chunk<true>(c, b, fin, (int)count, (int)polys, inverse, st);
+    } else if (c.mode == 2) {
+      launch_ntt_chunk<2>(c, b, fin, (int)count, (int)polys, inverse, st);
+    } else if (c.mode == 1) {
+      launch_ntt_chunk<1>(c, b, fin, (int)count, (int)polys, inverse, st);
     } else {
-      launch_ntt_chunk<false>(c, b, fin, (int)count, (int)polys, inverse, st);
+      launch_ntt_chunk<0>(c, b, fin, (int)count, (int)polys, inverse, st);
     }
   }
 }
@@ -540,7 +542,7 @@ void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, bo
 void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
               const std::vector<uint16_t> &slots, size_t polys, u64 src_stride, u64 dst_stride,
               cudaStream_t st, bool lazy_out = false) {
-  lazy_out = lazy_out && c.lazy && c.logn >= 12;
+  lazy_out = lazy_out && c.mode >= 1 && c.logn >= 12;
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   b200::ConvArgs a{};
   a.plan = p.device;
@@ -1024,7 +1026,8 @@ int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const
       require(std::find(c->mod.begin(), c->mod.end(), mq) == c->mod.end(), "duplicate Q/P modulus");
       c->mod.push_back(mq);
       c->psi.push_back(ps);
-      if (mq >= (u64(1) << 62)) c->lazy = false;
+      if (mq >= (u64(1) << 61)) c->mode = std::min(c->mode, 1);
+      if (mq >= (u64(1) << 62)) c->mode = 0;
     }
     const size_t T = m + k;
     std::vector<b200::TowerConsts> tc(T);

@@ -141,7 +141,7 @@ struct ColGeom {
   }
 };
 
-template <int LOGN, bool LAZY>
+template <int LOGN, int MODE>
 __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b,
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
-      ct_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+      ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
     }
   }
   if constexpr (G::LR > 4) {
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b,
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
         const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
-        ct_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+        ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
       }
     }
     __syncthreads();
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b,
   store_block<G::R, G::COLS, G::COLS, false>(v.dst + col0, tile, N >> G::LR);
 }
 
-template <int LOGN, bool LAZY>
+template <int LOGN, int MODE>
 __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b,
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
         const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
-        gs_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+        gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
       }
     }
     __syncthreads();
@@ -241,12 +241,12 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b,
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
-      gs_butterfly<LAZY>(x[e], x[e + d], w.x, w.y, q, q2);
+      gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
     }
   }
   const Shoup ninv = v.c->ninv, last = v.c->last_inv;
 #pragma unroll
-  for (int e = 0; e < 8; ++e) gs_last<LAZY>(x[e], x[e + 8], ninv, last, q, q2);
+  for (int e = 0; e < 8; ++e) gs_last<MODE>(x[e], x[e + 8], ninv, last, q, q2);
   __syncthreads();
 #pragma unroll
   for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b,
 // (one pad word per 16) so both mappings are bank-conflict free.
 __device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
 
-template <int LOGN, bool LAZY>
+template <int LOGN, int MODE>
 __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
   __shared__ u64 tile[16 * kRowPad];
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b,
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-      ct_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+      ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
     }
   }
   __syncwarp();
@@ -301,12 +301,12 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b,
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
-      ct_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+      ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
     }
   }
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
-    if constexpr (LAZY) x[e] = reduce4(x[e], q, q2);
+    x[e] = reduce_final<MODE>(x[e], q, q2);
     my[pad_col(u * 16 + e)] = x[e];
   }
   __syncthreads();
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b,
   }
 }
 
-template <int LOGN, bool LAZY>
+template <int LOGN, int MODE>
 __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
   __shared__ u64 tile[16 * kRowPad];
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_row(NttBatch b,
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
-      gs_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+      gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
     }
   }
   __syncwarp();
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_row(NttBatch b,
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-      gs_butterfly<LAZY>(x[e], x[e + d], w.w, w.wq, q, q2);
+      gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
     }
   }
 #pragma unroll

@@ -60,7 +60,7 @@ constexpr int col_smem_bytes() {
   return 2 * kTileWords * 8 + 2 * (1 << (LOGN - 8)) * 16;
 }
 
-template <int LOGN, bool LAZY, bool INV>
+template <int LOGN, int MODE, bool INV>
 __global__ void __launch_bounds__(kNttThreads, 3) ntt_col_ps(NttBatch b, DeviceTables T, uint32_t slots,
                                                              uint32_t total) {
   using G = ColGeom<LOGN>;
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_col_ps(NttBatch b, DeviceT
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
           const ulonglong2 t = tw[(1 << s) + (e >> (4 - s))];
-          ct_butterfly<LAZY>(x[e], x[e + d], t.x, t.y, q, q2);
+          ct_butterfly<MODE>(x[e], x[e + d], t.x, t.y, q, q2);
         }
       }
       if constexpr (G::LR > 4) {
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_col_ps(NttBatch b, DeviceT
           for (int e = 0; e < 16; ++e) {
             if (e & d) continue;
             const ulonglong2 t = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
-            ct_butterfly<LAZY>(x[e], x[e + d], t.x, t.y, q, q2);
+            ct_butterfly<MODE>(x[e], x[e + d], t.x, t.y, q, q2);
           }
         }
         __syncthreads();
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_col_ps(NttBatch b, DeviceT
           for (int e = 0; e < 16; ++e) {
             if (e & d) continue;
             const ulonglong2 t = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
-            gs_butterfly<LAZY>(x[e], x[e + d], t.x, t.y, q, q2);
+            gs_butterfly<MODE>(x[e], x[e + d], t.x, t.y, q, q2);
           }
         }
         __syncthreads();
@@ -168,12 +168,12 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_col_ps(NttBatch b, DeviceT
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
           const ulonglong2 t = tw[(1 << s) + (e >> (4 - s))];
-          gs_butterfly<LAZY>(x[e], x[e + d], t.x, t.y, q, q2);
+          gs_butterfly<MODE>(x[e], x[e + d], t.x, t.y, q, q2);
         }
       }
       const Shoup ninv = v.c->ninv, last = v.c->last_inv;
 #pragma unroll
-      for (int e = 0; e < 8; ++e) gs_last<LAZY>(x[e], x[e + 8], ninv, last, q, q2);
+      for (int e = 0; e < 8; ++e) gs_last<MODE>(x[e], x[e + 8], ninv, last, q, q2);
       __syncthreads();
 #pragma unroll
       for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
@@ -197,7 +197,7 @@ __device__ __forceinline__ int swz_word(int col) { return (swz_chunk(col >> 1) <
 
 constexpr int kRowPsSmem = 2 * kTileWords * 8;
 
-template <int LOGN, bool LAZY, bool INV>
+template <int LOGN, int MODE, bool INV>
 __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceTables T, uint32_t slots,
                                                              uint32_t total) {
   constexpr int LR = LOGN - 8;
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
           const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-          ct_butterfly<LAZY>(x[e], x[e + d], t.w, t.wq, q, q2);
+          ct_butterfly<MODE>(x[e], x[e + d], t.w, t.wq, q, q2);
         }
       }
       __syncwarp();
@@ -266,14 +266,14 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
           const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
-          ct_butterfly<LAZY>(x[e], x[e + d], t.w, t.wq, q, q2);
+          ct_butterfly<MODE>(x[e], x[e + d], t.w, t.wq, q, q2);
         }
       }
 #pragma unroll
       for (int e = 0; e < 16; e += 2) {
         ulonglong2 p;
-        p.x = LAZY ? reduce4(x[e], q, q2) : x[e];
-        p.y = LAZY ? reduce4(x[e + 1], q, q2) : x[e + 1];
+        p.x = reduce_final<MODE>(x[e], q, q2);
+        p.y = reduce_final<MODE>(x[e + 1], q, q2);
         *reinterpret_cast<ulonglong2 *>(my + swz_chunk(u * 8 + e / 2) * 2) = p;
       }
     } else {
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
           const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
-          gs_butterfly<LAZY>(x[e], x[e + d], t.w, t.wq, q, q2);
+          gs_butterfly<MODE>(x[e], x[e + d], t.w, t.wq, q, q2);
         }
       }
       __syncwarp();
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
           const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-          gs_butterfly<LAZY>(x[e], x[e + d], t.w, t.wq, q, q2);
+          gs_butterfly<MODE>(x[e], x[e + d], t.w, t.wq, q, q2);
         }
       }
 #pragma unroll

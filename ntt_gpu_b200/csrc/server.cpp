@@ -12,8 +12,10 @@
 //    device (a depth above 1 queues the next wave behind the running one);
 //  - workspace comes from the device's stream-ordered pool and is returned in
 //    stream order after the wave;
-//  - a host callback at the end of each wave's stream work records completion,
-//    so latency is measured from submission to the GPU finishing the wave.
+//  - an event recorded after each wave marks its completion; the scheduler
+//    polls the events of waves in flight (every 20 us while any is in flight),
+//    so latency runs from submission to the observed GPU completion, and no
+//    host callback ever stalls a lane's stream.
 // The reference serves one request per Session transaction (src/resident.cpp,
 // include/ntt/openfhe_hybrid_adapter.hpp:163-181) and has no server; the
 // admission budget follows its Limits/Reservation model (src/resident.cpp:10-28).
@@ -51,14 +53,12 @@ struct Ticket {
   int lane = -1;
 };
 
-// One launched wave; its address is the completion callback's argument.
+// One launched wave and the event recorded after its work.
 struct Wave {
-  ntt_b200_server_s *srv = nullptr;
   int lane = -1;
   std::vector<uint64_t> ids;
   size_t bytes = 0;
-  bool finished = false;
-  double t_finished = 0;
+  cudaEvent_t done = nullptr;
 };
 
 struct Lane {
@@ -75,7 +75,8 @@ struct ntt_b200_server_s {
   std::deque<uint64_t> pending;
   std::unordered_map<uint64_t, Ticket> tickets;
   std::vector<Lane> lanes;
-  std::unordered_map<Wave *, std::unique_ptr<Wave>> waves_in_flight;
+  std::vector<std::unique_ptr<Wave>> waves_in_flight;
+  std::vector<cudaEvent_t> event_pool;
   int depth = 1;
   uint64_t next_id = 1;
   size_t in_use = 0, peak_in_use = 0;
@@ -87,36 +88,46 @@ struct ntt_b200_server_s {
   uint64_t waves = 0, wave_requests = 0;
   double first_submit = 0, last_done = 0, queue_us = 0;
 
-  // Runs on the CUDA callback thread when a wave finished on the GPU. It
-  // makes no CUDA calls.
-  static void CUDART_CB on_wave_done(void *p) {
-    auto *w = static_cast<Wave *>(p);
-    const double t = now_us();
-    std::lock_guard<std::mutex> lock(w->srv->mu);
-    w->finished = true;
-    w->t_finished = t;
-    w->srv->cv_sched.notify_all();
+  cudaEvent_t take_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    return e;
   }
 
-  // Retire finished waves (lock held).
+  // Retire waves whose completion event has fired (lock held).
   void retire() {
     for (auto it = waves_in_flight.begin(); it != waves_in_flight.end();) {
-      Wave &w = *it->second;
-      if (!w.finished) {
+      Wave &w = **it;
+      const cudaError_t q = cudaEventQuery(w.done);
+      if (q == cudaErrorNotReady) {
         ++it;
         continue;
       }
+      const double t_done = now_us();
+      const bool ok = q == cudaSuccess;
+      const std::string why = ok ? "" : std::string("CUDA: wave: ") + cudaGetErrorString(q);
       for (uint64_t id : w.ids) {
         auto t = tickets.find(id);
         if (t == tickets.end()) continue;
+        if (!ok) {
+          fail_ticket(id, NTT_B200_ERR_CUDA, why);
+          continue;
+        }
         t->second.status = NTT_B200_OK;
-        t->second.t_done = w.t_finished;
-        latencies_us.push_back(w.t_finished - t->second.t_submit);
+        t->second.t_done = t_done;
+        latencies_us.push_back(t_done - t->second.t_submit);
         queue_us += t->second.t_launch - t->second.t_submit;
-        last_done = std::max(last_done, w.t_finished);
+        last_done = std::max(last_done, t_done);
       }
+      if (!ok && fatal.empty()) fatal = why;
       in_use -= w.bytes;
       lanes[w.lane].inflight -= 1;
+      event_pool.push_back(w.done);
       it = waves_in_flight.erase(it);
       cv_done.notify_all();
     }
@@ -199,11 +210,11 @@ struct ntt_b200_server_s {
       tk.lane = lane;
     }
     auto owned = std::make_unique<Wave>();
-    Wave *wv = owned.get();
-    wv->srv = this;
-    wv->lane = lane;
-    wv->ids = wave;
-    wv->bytes = need;
+    owned->lane = lane;
+    owned->ids = wave;
+    owned->bytes = need;
+    owned->done = take_event();
+    cudaEvent_t done = owned->done;
     lanes[lane].inflight += 1;
     in_use += need;
     peak_in_use = std::max(peak_in_use, in_use);
@@ -212,7 +223,7 @@ struct ntt_b200_server_s {
     int rc = NTT_B200_OK;
     std::string why;
     void *ws = nullptr;
-    cudaError_t e = cudaMallocAsync(&ws, std::max<size_t>(need, 256), stream);
+    cudaError_t e = done ? cudaMallocAsync(&ws, std::max<size_t>(need, 256), stream) : cudaErrorMemoryAllocation;
     if (e != cudaSuccess) {
       rc = NTT_B200_ERR_CUDA;
       why = std::string("CUDA: cudaMallocAsync: ") + cudaGetErrorString(e);
@@ -221,10 +232,10 @@ struct ntt_b200_server_s {
       if (rc != NTT_B200_OK) why = ntt_b200_last_error();
       cudaFreeAsync(ws, stream);
       if (rc == NTT_B200_OK) {
-        e = cudaLaunchHostFunc(stream, &ntt_b200_server_s::on_wave_done, wv);
+        e = cudaEventRecord(done, stream);
         if (e != cudaSuccess) {
           rc = NTT_B200_ERR_CUDA;
-          why = std::string("CUDA: cudaLaunchHostFunc: ") + cudaGetErrorString(e);
+          why = std::string("CUDA: cudaEventRecord: ") + cudaGetErrorString(e);
         }
       }
     }
@@ -232,11 +243,12 @@ struct ntt_b200_server_s {
     if (rc != NTT_B200_OK) {
       lanes[lane].inflight -= 1;
       in_use -= need;
+      if (done) event_pool.push_back(done);
       for (uint64_t id : wave) fail_ticket(id, rc, why);
       if (rc == NTT_B200_ERR_CUDA && fatal.empty()) fatal = why;
       return true;
     }
-    waves_in_flight.emplace(wv, std::move(owned));
+    waves_in_flight.push_back(std::move(owned));
     waves += 1;
     wave_requests += wave.size();
     return true;
@@ -249,7 +261,10 @@ struct ntt_b200_server_s {
       retire();
       while (launch_one(lock)) retire();
       if (stopping && pending.empty() && !any_busy()) break;
-      cv_sched.wait(lock);
+      if (any_busy())
+        cv_sched.wait_for(lock, std::chrono::microseconds(20));  // poll the waves in flight
+      else
+        cv_sched.wait(lock);
     }
   }
 };
@@ -443,6 +458,7 @@ int ntt_b200_server_destroy(ntt_b200_server srv) {
       cudaStreamSynchronize(l.stream);
       cudaStreamDestroy(l.stream);
     }
+    for (cudaEvent_t e : srv->event_pool) cudaEventDestroy(e);
     delete srv;
     return NTT_B200_OK;
   });

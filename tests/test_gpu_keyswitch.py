@@ -136,3 +136,21 @@ def test_full_size_golden_digests(lib, orc):
         assert gc.sha(nb.to_host(out)) == d[f"ntt_{name}_forward"]
         g.ntt(out, nb.to_device(x), [0], inverse=True)
         assert gc.sha(nb.to_host(out)) == d[f"ntt_{name}_inverse"]
+
+
+@pytest.mark.parametrize("q_bits,p_bits", [(60, 61), (61, 62)])
+def test_keyswitch_with_wide_towers(lib, orc, q_bits, p_bits):
+    """Whole key switch (digits, MAC, rotation, ModDown) with towers just below
+    2^61 (fast butterflies at the top of their range) and in [2^61, 2^62) (lazy)."""
+    ctx = synthetic_context(orc, 8192, 6, 3, 2, q_bits=q_bits, p_bits=p_bits)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka = full_keys(orc, ctx, 61)
+    for level in (6, 3):
+        x = orc.lcg(ctx.n, ctx.q[:level], 70 + level)
+        c0 = orc.lcg(ctx.n, ctx.q[:level], 71 + level)
+        ob, oa = nb.empty((level, ctx.n)), nb.empty((level, ctx.n))
+        g.keyswitch(level, ob, oa, nb.to_device(x), nb.to_device(kb), nb.to_device(ka),
+                    g.workspace(nb.OP_KEYSWITCH, level), c0=nb.to_device(c0), automorphism=25)
+        wb, wa = orc.keyswitch(ctx, level, x, kb, ka, c0, 25)
+        np.testing.assert_array_equal(nb.to_host(ob), wb)
+        np.testing.assert_array_equal(nb.to_host(oa), wa)

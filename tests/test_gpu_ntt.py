@@ -93,3 +93,27 @@ def test_batched_polys_with_stride(lib, orc):
     for p in range(polys):
         np.testing.assert_array_equal(got[p, :len(q)], orc.ntt(buf[p, :len(q)], q, psi))
         np.testing.assert_array_equal(got[p, len(q)], 0)  # the gap tower is untouched
+
+
+@pytest.mark.parametrize("bits", [[61], [62], [61, 62], [59, 61]])
+@pytest.mark.parametrize("logn", [12, 16])
+def test_butterfly_mode_boundaries(lib, orc, bits, logn):
+    """Moduli just below 2^61 (fast approximate-quotient butterflies, values up to
+    8q), in [2^61, 2^62) (Harvey lazy butterflies) and mixed: exact results, with
+    all-(q-1) inputs driving every stage to the top of its range."""
+    n = 1 << logn
+    q = []
+    for b in bits:
+        q += [v for v in orc.find_primes(n, 2, b) if v not in q][:2]
+    psi = [orc.find_psi(v, n) for v in q]
+    ctx = nb.Context(n, q, psi)
+    ids = list(range(len(q)))
+    for x in (orc.lcg(n, q, 5 + logn), np.array([[v - 1] * n for v in q], dtype=np.uint64)):
+        out = nb.empty(x.shape)
+        ctx.ntt(out, nb.to_device(x), ids)
+        np.testing.assert_array_equal(nb.to_host(out), orc.ntt(x, q, psi))
+        back = nb.empty(x.shape)
+        ctx.ntt(back, out, ids, inverse=True)
+        np.testing.assert_array_equal(nb.to_host(back), x)
+        ctx.ntt(out, nb.to_device(x), ids, inverse=True)
+        np.testing.assert_array_equal(nb.to_host(out), orc.ntt(x, q, psi, inverse=True))
