@@ -138,6 +138,7 @@ struct HostConvPlan {
   b200::ConvPlan *device = nullptr;
   int s = 0, t = 0;
   bool wide = false;
+  bool limb = false;  // all moduli < 2^60 and s <= 8: the 30-bit-limb kernel applies
 };
 }  // namespace
 
@@ -214,6 +215,7 @@ struct ntt_b200_context_s {
     hp.t = t;
     const u128 prod = (u128)(max_src - 1) * (max_tgt - 1);
     hp.wide = prod > (~(u128)0) / (u128)s;
+    hp.limb = s <= 8 && max_src < (u64(1) << 60) && max_tgt < (u64(1) << 60);
     DeviceGuard guard(device);
     CUDA_CHECK(cudaMalloc(&hp.device, sizeof(b200::ConvPlan)));
     CUDA_CHECK(cudaMemcpy(hp.device, plan.get(), sizeof(b200::ConvPlan), cudaMemcpyHostToDevice));
@@ -529,8 +531,26 @@ std::vector<uint16_t> qp_ids(const Ctx &c, size_t level) {
 }
 
 // ---- conversion launches ---------------------------------------------------------
+// NTT_B200_CONV_LIMBS=0 selects the 128-bit-accumulator kernel for every plan
+// (the two kernels give identical results; the switch exists for measurement).
+bool conv_limbs_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("NTT_B200_CONV_LIMBS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 template <int MAXS>
 void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, bool lazy_out, cudaStream_t st) {
+  if constexpr (MAXS <= 8) {
+    if (p.limb && conv_limbs_enabled()) {
+      if (lazy_out)
+        b200::conv_limb_kernel<MAXS, true><<<grid, b200::kEwThreads, 0, st>>>(a);
+      else
+        b200::conv_limb_kernel<MAXS, false><<<grid, b200::kEwThreads, 0, st>>>(a);
+      return;
+    }
+  }
   if (p.wide)
     b200::conv_kernel<MAXS, true, false><<<grid, b200::kEwThreads, 0, st>>>(a);
   else if (lazy_out)

@@ -80,6 +80,69 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
   }
 }
 
+// Same switch when every source and target modulus is below 2^60 and s <= 8:
+// with y = y1*2^30 + y0 and Bhat = h1*2^30 + h0 (30-bit limbs), the exact sum
+// is H*2^60 + C*2^30 + L with L = sum y0*h0, H = sum y1*h1 and
+// C = sum (y0*h1 + y1*h0) = sum (y0+y1)(h0+h1) - L - H. Each term costs three
+// 32x32->64 multiply-adds and no carry handling: L, H < 8*2^60 and C < 8*2^61
+// fit in 64 bits, and the (y0+y1)(h0+h1) sum may wrap because only its
+// difference C is used. The result equals conv_kernel's bit for bit.
+template <int MAXS, bool LAZY_OUT>
+__global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
+  constexpr uint32_t kMask30 = (1u << 30) - 1;
+  __shared__ uint32_t h0s[MAXS * kMaxConvTargets], h1s[MAXS * kMaxConvTargets], hss[MAXS * kMaxConvTargets];
+  __shared__ Reducer red[kMaxConvTargets];
+  __shared__ u64 sq[MAXS];
+  __shared__ Shoup sinv[MAXS];
+  const ConvPlan &p = *a.plan;
+  const int s = p.s;
+  const int t0 = blockIdx.y * a.targets_per_block;
+  const int t1 = min(p.t, t0 + a.targets_per_block);
+  const int nt = t1 - t0;
+  for (int i = threadIdx.x; i < s * nt; i += blockDim.x) {
+    const int j = i / nt, t = i % nt;
+    const u64 h = p.hat[j * p.t + t0 + t];
+    const uint32_t lo = (uint32_t)h & kMask30, hi = (uint32_t)(h >> 30);
+    h0s[j * nt + t] = lo;
+    h1s[j * nt + t] = hi;
+    hss[j * nt + t] = lo + hi;
+  }
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) red[t] = p.tgt[t0 + t];
+  for (int j = threadIdx.x; j < s; j += blockDim.x) {
+    sq[j] = p.src_q[j];
+    sinv[j] = p.src_inv[j];
+  }
+  __syncthreads();
+  const u64 n = u64(1) << a.logn;
+  const u64 k = u64(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const u64 *src = a.src + blockIdx.z * a.src_poly_stride;
+  u64 *dst = a.dst + blockIdx.z * a.dst_poly_stride;
+  uint32_t y0[MAXS], y1[MAXS], ys[MAXS];
+#pragma unroll
+  for (int j = 0; j < MAXS; ++j) {
+    const u64 y = j < s ? shoup_canon(src[j * n + k], sinv[j].w, sinv[j].wq, sq[j]) : 0;
+    y0[j] = (uint32_t)y & kMask30;
+    y1[j] = (uint32_t)(y >> 30);
+    ys[j] = y0[j] + y1[j];
+  }
+  for (int t = 0; t < nt; ++t) {
+    u64 lo = 0, hi = 0, mid = 0;
+#pragma unroll
+    for (int j = 0; j < MAXS; ++j) {
+      if (j < s) {
+        lo += (u64)y0[j] * h0s[j * nt + t];
+        hi += (u64)y1[j] * h1s[j * nt + t];
+        mid += (u64)ys[j] * hss[j * nt + t];
+      }
+    }
+    const u64 cross = mid - lo - hi;
+    Acc128 v;
+    v.v = ((u128)hi << 60) + ((u128)cross << 30) + lo;
+    dst[u64(a.slot[t0 + t]) * n + k] = reduce_out<LAZY_OUT>(v, red[t]);
+  }
+}
+
 // ---- ModDown tail: (l - r) * [P^-1]_q  (resident_conversion.hpp:45-49) ---------
 struct CorrectArgs {
   u64 *dst, *dst_odd;  // dst_odd set: polynomial z writes (z odd ? dst_odd : dst) + (z / 2) * stride
