@@ -202,7 +202,8 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
  * ticket completes. A scheduler thread forms waves of the oldest pending
  * request's (context, level) class, up to max_batch, and launches each on the
  * least-loaded lane (a CUDA stream with fewer than `depth` waves in flight)
- * once its workspace fits hbm_budget_bytes next to the waves in flight: requests arriving while others run join the next
+ * once its workspace fits the lane's arena, grown within hbm_budget_bytes
+ * (the sum of all lanes' arenas; idle lanes give theirs back when needed): requests arriving while others run join the next
  * wave as lanes and memory free up, and waves on different lanes overlap on
  * the device. Each result equals the request run alone. The reference has no
  * server (one request per Session transaction, src/resident.cpp); admission
@@ -213,7 +214,7 @@ typedef struct ntt_b200_server_config {
   int lanes;      /* CUDA streams that run waves concurrently, 1..16 */
   int max_batch;  /* requests per wave, 1..1024 */
   int depth;      /* waves in flight per lane, 1..8 (0 = 1); >1 queues the next wave behind the running one */
-  size_t hbm_budget_bytes; /* workspace of all in-flight waves */
+  size_t hbm_budget_bytes; /* sum of the lanes' workspace arenas */
 } ntt_b200_server_config;
 typedef struct ntt_b200_ticket_info {
   int status;          /* NTT_B200_OK or the request's error */
@@ -228,7 +229,7 @@ typedef struct ntt_b200_server_report {
   double mean_wave, p50_ms, p99_ms, max_ms;
   double throughput;   /* completed / (last completion - first submission), per second */
   double mean_queue_ms; /* submission -> wave launch, mean */
-  size_t peak_bytes, in_flight_bytes;
+  size_t peak_bytes, in_flight_bytes; /* workspace arenas held by the lanes: peak and now */
 } ntt_b200_server_report;
 const char *ntt_b200_server_last_error(void);
 int ntt_b200_server_create(ntt_b200_server *out, const ntt_b200_server_config *cfg);

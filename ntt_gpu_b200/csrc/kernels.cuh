@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kEwThreads) conv_kernel(ConvArgs a) {
 template <int MAXS, bool LAZY_OUT>
 __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
   constexpr uint32_t kMask30 = (1u << 30) - 1;
-  __shared__ uint32_t h0s[MAXS * kMaxConvTargets], h1s[MAXS * kMaxConvTargets], hss[MAXS * kMaxConvTargets];
+  __shared__ uint4 hl[MAXS * kMaxConvTargets];  // (h0, h1, h0 + h1, 0) per (source, target)
   __shared__ Reducer red[kMaxConvTargets];
   __shared__ u64 sq[MAXS];
   __shared__ Shoup sinv[MAXS];
@@ -103,9 +103,7 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
     const int j = i / nt, t = i % nt;
     const u64 h = p.hat[j * p.t + t0 + t];
     const uint32_t lo = (uint32_t)h & kMask30, hi = (uint32_t)(h >> 30);
-    h0s[j * nt + t] = lo;
-    h1s[j * nt + t] = hi;
-    hss[j * nt + t] = lo + hi;
+    hl[j * nt + t] = make_uint4(lo, hi, lo + hi, 0);
   }
   for (int t = threadIdx.x; t < nt; t += blockDim.x) red[t] = p.tgt[t0 + t];
   for (int j = threadIdx.x; j < s; j += blockDim.x) {
@@ -126,20 +124,41 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
     y1[j] = (uint32_t)(y >> 30);
     ys[j] = y0[j] + y1[j];
   }
-  for (int t = 0; t < nt; ++t) {
+  auto finish = [&](u64 lo, u64 hi, u64 mid, int t) {
+    Acc128 v;
+    v.v = ((u128)hi << 60) + ((u128)(mid - lo - hi) << 30) + lo;
+    dst[u64(a.slot[t0 + t]) * n + k] = reduce_out<LAZY_OUT>(v, red[t]);
+  };
+  int t = 0;
+  for (; t + 1 < nt; t += 2) {
+    u64 lo0 = 0, hi0 = 0, mid0 = 0, lo1 = 0, hi1 = 0, mid1 = 0;
+#pragma unroll
+    for (int j = 0; j < MAXS; ++j) {
+      if (j < s) {
+        const uint4 h = hl[j * nt + t], g = hl[j * nt + t + 1];
+        lo0 += (u64)y0[j] * h.x;
+        hi0 += (u64)y1[j] * h.y;
+        mid0 += (u64)ys[j] * h.z;
+        lo1 += (u64)y0[j] * g.x;
+        hi1 += (u64)y1[j] * g.y;
+        mid1 += (u64)ys[j] * g.z;
+      }
+    }
+    finish(lo0, hi0, mid0, t);
+    finish(lo1, hi1, mid1, t + 1);
+  }
+  if (t < nt) {
     u64 lo = 0, hi = 0, mid = 0;
 #pragma unroll
     for (int j = 0; j < MAXS; ++j) {
       if (j < s) {
-        lo += (u64)y0[j] * h0s[j * nt + t];
-        hi += (u64)y1[j] * h1s[j * nt + t];
-        mid += (u64)ys[j] * hss[j * nt + t];
+        const uint4 h = hl[j * nt + t];
+        lo += (u64)y0[j] * h.x;
+        hi += (u64)y1[j] * h.y;
+        mid += (u64)ys[j] * h.z;
       }
     }
-    const u64 cross = mid - lo - hi;
-    Acc128 v;
-    v.v = ((u128)hi << 60) + ((u128)cross << 30) + lo;
-    dst[u64(a.slot[t0 + t]) * n + k] = reduce_out<LAZY_OUT>(v, red[t]);
+    finish(lo, hi, mid, t);
   }
 }
 

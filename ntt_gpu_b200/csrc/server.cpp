@@ -10,8 +10,10 @@
 //    already in flight, so requests that arrive while others run are admitted
 //    as lanes and memory free up, and waves on different lanes overlap on the
 //    device (a depth above 1 queues the next wave behind the running one);
-//  - workspace comes from the device's stream-ordered pool and is returned in
-//    stream order after the wave;
+//  - each lane owns a workspace arena that its waves reuse in stream order; an
+//    arena only grows (stream-ordered free + allocation on its own stream), the
+//    sum of all arenas stays within the HBM budget, and idle lanes give their
+//    arenas back when a wave needs the room;
 //  - an event recorded after each wave marks its completion; the scheduler
 //    polls the events of waves in flight (every 20 us while any is in flight),
 //    so latency runs from submission to the observed GPU completion, and no
@@ -64,6 +66,8 @@ struct Wave {
 struct Lane {
   cudaStream_t stream = nullptr;
   int inflight = 0;  // waves enqueued on this stream and not yet retired
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
 };
 
 }  // namespace
@@ -125,7 +129,6 @@ struct ntt_b200_server_s {
         last_done = std::max(last_done, t_done);
       }
       if (!ok && fatal.empty()) fatal = why;
-      in_use -= w.bytes;
       lanes[w.lane].inflight -= 1;
       event_pool.push_back(w.done);
       it = waves_in_flight.erase(it);
@@ -177,8 +180,10 @@ struct ntt_b200_server_s {
       wave.push_back(id);
       reqs.push_back(t.req);
     }
-    // Shrink the wave until its workspace fits the budget left.
+    // Shrink the wave until it fits the lane's arena, grown within the budget
+    // (idle lanes' arenas are released first when the room is needed).
     size_t need = 0;
+    std::vector<int> release;  // idle lanes whose arenas this wave takes over
     while (true) {
       if (ntt_b200_keyswitch_requests_workspace(ctx, reqs.data(), reqs.size(), &need) != NTT_B200_OK) {
         // Requests are validated at submission; a failure here fails the wave.
@@ -187,14 +192,28 @@ struct ntt_b200_server_s {
         erase_pending(wave);
         return true;
       }
-      if (in_use + need <= cfg.hbm_budget_bytes) break;
+      const size_t mine = lanes[lane].arena_bytes;
+      if (need <= mine) break;
+      size_t others = in_use - mine, idle = 0;
+      release.clear();
+      for (size_t i = 0; i < lanes.size(); ++i)
+        if ((int)i != lane && lanes[i].inflight == 0 && lanes[i].arena_bytes) {
+          idle += lanes[i].arena_bytes;
+          release.push_back((int)i);
+        }
+      if (others + need <= cfg.hbm_budget_bytes) {
+        release.clear();
+        break;
+      }
+      if (others - idle + need <= cfg.hbm_budget_bytes) break;
+      release.clear();
       if (reqs.size() == 1) {
         if (need > cfg.hbm_budget_bytes) {
           fail_ticket(wave[0], NTT_B200_ERR_WORKSPACE, "request workspace exceeds the server's HBM budget");
           erase_pending(wave);
           return true;
         }
-        return false;  // wait for in-flight waves to release memory
+        return false;  // wait for in-flight waves to free their lanes
       }
       const size_t keep = reqs.size() / 2;
       reqs.resize(keep);
@@ -212,25 +231,44 @@ struct ntt_b200_server_s {
     auto owned = std::make_unique<Wave>();
     owned->lane = lane;
     owned->ids = wave;
-    owned->bytes = need;
+    owned->bytes = need;  // informational: the lane's arena holds the memory
     owned->done = take_event();
     cudaEvent_t done = owned->done;
     lanes[lane].inflight += 1;
-    in_use += need;
+    // Arena changes happen under the lock, in stream order on each lane's own
+    // stream (frees and allocations are stream-ordered, never synchronous).
+    cudaError_t e = done ? cudaSuccess : cudaErrorMemoryAllocation;
+    for (int i : release) {
+      if (e == cudaSuccess) e = cudaFreeAsync(lanes[i].arena, lanes[i].stream);
+      in_use -= lanes[i].arena_bytes;
+      lanes[i].arena = nullptr;
+      lanes[i].arena_bytes = 0;
+    }
+    Lane &ln = lanes[lane];
+    if (e == cudaSuccess && need > ln.arena_bytes) {
+      if (ln.arena) e = cudaFreeAsync(ln.arena, ln.stream);
+      in_use -= ln.arena_bytes;
+      ln.arena = nullptr;
+      ln.arena_bytes = 0;
+      if (e == cudaSuccess) e = cudaMallocAsync(&ln.arena, need, ln.stream);
+      if (e == cudaSuccess) {
+        ln.arena_bytes = need;
+        in_use += need;
+      }
+    }
     peak_in_use = std::max(peak_in_use, in_use);
-    const cudaStream_t stream = lanes[lane].stream;
+    const cudaStream_t stream = ln.stream;
+    void *ws = ln.arena;
+    const size_t ws_bytes = ln.arena_bytes;
     lock.unlock();
     int rc = NTT_B200_OK;
     std::string why;
-    void *ws = nullptr;
-    cudaError_t e = done ? cudaMallocAsync(&ws, std::max<size_t>(need, 256), stream) : cudaErrorMemoryAllocation;
     if (e != cudaSuccess) {
       rc = NTT_B200_ERR_CUDA;
-      why = std::string("CUDA: cudaMallocAsync: ") + cudaGetErrorString(e);
+      why = std::string("CUDA: lane arena: ") + cudaGetErrorString(e);
     } else {
-      rc = ntt_b200_keyswitch_requests(ctx, reqs.data(), reqs.size(), ws, need, stream);
+      rc = ntt_b200_keyswitch_requests(ctx, reqs.data(), reqs.size(), ws, ws_bytes, stream);
       if (rc != NTT_B200_OK) why = ntt_b200_last_error();
-      cudaFreeAsync(ws, stream);
       if (rc == NTT_B200_OK) {
         e = cudaEventRecord(done, stream);
         if (e != cudaSuccess) {
@@ -242,7 +280,6 @@ struct ntt_b200_server_s {
     lock.lock();
     if (rc != NTT_B200_OK) {
       lanes[lane].inflight -= 1;
-      in_use -= need;
       if (done) event_pool.push_back(done);
       for (uint64_t id : wave) fail_ticket(id, rc, why);
       if (rc == NTT_B200_ERR_CUDA && fatal.empty()) fatal = why;
@@ -455,6 +492,7 @@ int ntt_b200_server_destroy(ntt_b200_server srv) {
     }
     srv->sched.join();  // drains pending work first
     for (Lane &l : srv->lanes) {
+      if (l.arena) cudaFreeAsync(l.arena, l.stream);
       cudaStreamSynchronize(l.stream);
       cudaStreamDestroy(l.stream);
     }
