@@ -325,7 +325,8 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
             srv = nb.Server(device=device, **cfg)
             count = max(64, min(400, int(rate * 0.12)))
             jobs = [(w.ctx, w.request(nb, LEVEL, "switch", 0, i)) for i in range(count)]
-            serve_poisson(nb, srv, jobs[:16], rate, seed + 1)  # warm-up
+            # Warm-up: a burst sizes every lane's workspace arena for full waves.
+            serve_poisson(nb, srv, jobs[:2 * BATCH * cfg["lanes"]], 1e7, seed + 1)
             row[name] = serve_poisson(nb, srv, jobs, rate, seed)
             srv.close()
         head.append(row)
@@ -367,6 +368,7 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
         for name, cfg in legs:
             srv = nb.Server(device=device, **cfg)
             jobs = mixed_jobs(max(100, min(600, int(rate * 0.25))), seed + 7)
+            serve_poisson(nb, srv, burst[:2 * BATCH * cfg["lanes"]], 1e7, seed + 6)  # warm-up burst
             row[name] = serve_poisson(nb, srv, jobs, rate, seed + 8)
             srv.close()
         mixed.append(row)
