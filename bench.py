@@ -231,6 +231,88 @@ def run_reference(args, rank, world):
 
 
 # ---- GPU side ------------------------------------------------------------------------------------
+# ---- configs 1-3: NTT and conversion legs -------------------------------------------------------
+def config_legs(nb, device, peak):
+    """Config 1 (one 60-bit tower, forward + inverse), config 2 (8 x 32 towers, forward + inverse,
+    direct launches and CUDA-graph replay) and config 3 (fused digits and ModDown at L = 24)."""
+    import torch
+
+    from ntt_gpu_b200.params import find_primes, find_psi, synthetic_params, uniform_residues
+    W = 8 * N
+
+    def timed(fn, iters):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(iters):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(device)
+        return e0.elapsed_time(e1) / iters
+
+    def leg(ms, nbytes, **extra):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        return dict({"ms": ms, "algorithmic_bytes": nbytes, "gb_s": gbs, "frac_of_measured_hbm": gbs / peak}, **extra)
+
+    out = {}
+    # config 1: the pinned OpenFHE 60-bit tower (q0, psi from the reference's pinned table).
+    q0, psi0 = 1152921504606584833, 18043022392882
+    c1 = nb.Context(N, [q0], [psi0], device=device)
+    x1 = nb.to_device(uniform_residues(N, [q0], SEED)[0], device)
+    y1 = torch.empty_like(x1)
+    ms = timed(lambda: (c1.ntt(y1, x1, [0]), c1.ntt(y1, y1, [0], inverse=True)), 200)
+    out["config1"] = leg(ms, 4 * W, workload="N=2^16, one 60-bit tower, forward then inverse (latency-bound)")
+    c1.close()
+    # config 2: 8 polynomials x 32 towers (16 x 50-bit and 16 x 60-bit, interleaved).
+    q = [v for pair in zip(find_primes(N, 16, 50), find_primes(N, 16, 60)) for v in pair]
+    c2 = nb.Context(N, q, [find_psi(v, N) for v in q], device=device)
+    x2 = nb.to_device(uniform_residues(N, q, SEED, polys=8), device)
+    y2 = torch.empty_like(x2)
+    ids = list(range(32))
+
+    def fwd_inv():
+        c2.ntt(y2, x2, ids, polys=8, poly_stride=32 * N)
+        c2.ntt(y2, y2, ids, polys=8, poly_stride=32 * N, inverse=True)
+
+    direct = timed(fwd_inv, 20)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        fwd_inv()
+    torch.cuda.synchronize(device)
+    with torch.cuda.graph(graph):
+        fwd_inv()
+    replay = timed(graph.replay, 20)
+    exact = bool(torch.equal(y2, x2))
+    nbytes = 8 * 32 * 2 * 2 * W
+    out["config2"] = {"workload": "N=2^16, 8 polynomials x 32 towers (16 x 50-bit + 16 x 60-bit), forward then "
+                                  "inverse; 512 MiB moved, larger than L2",
+                      "direct": leg(direct, nbytes), "graph_replay": leg(replay, nbytes),
+                      "roundtrip_exact": exact}
+    del graph
+    c2.close()
+    # config 3: fused INTT -> ModUp -> NTT (Hybrid digits) and INTT -> ModDown -> NTT at L = 24.
+    prm = synthetic_params(N, LEVEL, K_P, DNUM)
+    c3 = nb.Context(prm.n, prm.q, prm.q_psi, prm.p, prm.p_psi, prm.alpha, device)
+    c3.prepare(LEVEL)
+    T, beta = LEVEL + K_P, prm.digits(LEVEL)
+    xq = nb.to_device(uniform_residues(N, prm.q, SEED)[0], device)
+    xqp = nb.to_device(uniform_residues(N, prm.q + prm.p, SEED + 1)[0], device)
+    digits = torch.empty((beta, T, N), dtype=torch.int64, device=xq.device)
+    down = torch.empty((LEVEL, N), dtype=torch.int64, device=xq.device)
+    wsd, wsm = c3.workspace(nb.OP_DIGITS, LEVEL), c3.workspace(nb.OP_MOD_DOWN, LEVEL)
+    ms_d = timed(lambda: c3.hybrid_digits(LEVEL, digits, xq, wsd), 50)
+    ms_m = timed(lambda: c3.mod_down(LEVEL, down, xqp, wsm), 50)
+    out["config3"] = {"workload": "N=2^16, L=24 (55-bit), K=8 (60-bit), dnum=3, one polynomial per call",
+                      "mod_up_digits": leg(ms_d, W * (LEVEL + beta * T)),
+                      "mod_down": leg(ms_m, W * (2 * LEVEL + K_P))}
+    c3.close()
+    return out
+
+
 # ---- serving: seeded Poisson arrivals through the continuous-batching server ---------------------
 def device_residues(n, moduli, seed, polys, device):
     """[polys][towers][n] int64 tensor of residues in [0, q_t) from a seeded device generator."""
@@ -527,6 +609,7 @@ def run_ours(args, rank, world, local):
 
     line["e2e"] = e2e
     line["plain"] = plain
+    line["configs"] = config_legs(nb, device, peaks()[0])
     if not args.no_serving:
         line["serving"] = serving_legs(nb, device, value, plain["value"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -276,6 +276,16 @@ int ntt_b200_event_record(void *event, void *stream);
 int ntt_b200_event_query(void *event);
 int ntt_b200_event_synchronize(void *event);
 
+/* Launch tuning: named choices that never change a result (which NTT pass
+ * variant and register budget, which conversion kernel, conversion grid size).
+ * ntt_gpu_b200/autotune.py measures them on the device and writes
+ * ntt_gpu_b200/tuning.json; the Python loader applies it at load time. Values
+ * out of a tunable's range are refused. tuning_name(i) lists the names (NULL
+ * past the end). The reference has no tuning interface. */
+int ntt_b200_tuning_set(const char *name, int64_t value);
+int ntt_b200_tuning_get(const char *name, int64_t *value);
+const char *ntt_b200_tuning_name(size_t index);
+
 /* Allocation-free ModDown. For callers that must not allocate device memory:
  * hosts whose HBM is already owned by another caching allocator (a framework
  * process that has reserved the device), latency-critical request threads that

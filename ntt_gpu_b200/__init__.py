@@ -86,6 +86,9 @@ _SIGNATURES = {
     "ntt_b200_event_synchronize": ([_P], _I),
     "ntt_b200_mod_down_static_max_bytes": ([], _SZ),
     "ntt_b200_mod_down_static": ([_P, _SZ, _P, _P, _P], _I),
+    "ntt_b200_tuning_set": ([ctypes.c_char_p, ctypes.c_int64], _I),
+    "ntt_b200_tuning_get": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)], _I),
+    "ntt_b200_tuning_name": ([_SZ], ctypes.c_char_p),
     "ntt_b200_timing_enable": ([_I], _I),
     "ntt_b200_timing_reset": ([], _I),
     "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),
@@ -119,8 +122,12 @@ def make_request(level, src, out_b, out_a, key_b, key_a, c0=None, automorphism=0
                      _ptr(add_a), int(automorphism), int(level))
 
 
+TUNING = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
+
+
 def load(path: str = LIB):
-    """Load libntt_b200.so and bind every entry point of include/ntt_b200.h."""
+    """Load libntt_b200.so, bind every entry point of include/ntt_b200.h and
+    apply the autotuner's committed choices (tuning.json) if present."""
     global _lib
     if _lib is not None:
         return _lib
@@ -132,7 +139,32 @@ def load(path: str = LIB):
         fn.argtypes = args
         fn.restype = res
     _lib = lib
+    if os.path.exists(TUNING):
+        import json
+        with open(TUNING) as f:
+            for name, value in json.load(f).get("choices", {}).items():
+                tuning_set(name, value)
     return lib
+
+
+def tuning_names() -> list:
+    lib, out, i = load(), [], 0
+    while True:
+        name = lib.ntt_b200_tuning_name(i)
+        if not name:
+            return out
+        out.append(name.decode())
+        i += 1
+
+
+def tuning_set(name: str, value: int):
+    _check(load().ntt_b200_tuning_set(name.encode(), int(value)))
+
+
+def tuning_get(name: str) -> int:
+    v = ctypes.c_int64()
+    _check(load().ntt_b200_tuning_get(name.encode(), ctypes.byref(v)))
+    return int(v.value)
 
 
 def library():

@@ -335,6 +335,31 @@ struct NttFinal {
   const b200::Shoup *epi_pinv = nullptr;
 };
 
+// ---- tuning -------------------------------------------------------------------------
+// Launch choices that do not change any result, set by name through
+// ntt_b200_tuning_set (ntt_gpu_b200/autotune.py measures them on the device and
+// commits its choices to ntt_gpu_b200/tuning.json, which the loader applies).
+struct Tunable {
+  const char *name;
+  std::atomic<int64_t> value;
+  int64_t lo, hi;
+};
+Tunable g_tuning[] = {
+    {"ntt_persistent", {0}, 0, 1},     // persistent double-buffered NTT passes instead of one CTA per tile
+    {"ntt_minb_fwd_col", {4}, 3, 4},   // CTAs per SM the forward column pass is compiled for
+    {"ntt_minb_fwd_row", {4}, 3, 4},
+    {"ntt_minb_inv_row", {4}, 3, 4},
+    {"ntt_minb_inv_col", {4}, 3, 4},
+    {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
+    {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
+};
+Tunable *find_tunable(const char *name) {
+  for (auto &t : g_tuning)
+    if (name && std::strcmp(t.name, name) == 0) return &t;
+  return nullptr;
+}
+int64_t tuned(const char *name) { return find_tunable(name)->value.load(std::memory_order_relaxed); }
+
 // Persistent double-buffered passes (ntt_ps.cuh): grid = resident CTAs of the
 // device; per-device launch attributes are set once.
 int device_sms(int device) {
@@ -354,13 +379,7 @@ unsigned persistent_grid(Kernel kernel, int smem, uint32_t total, int device, in
   const uint64_t resident = uint64_t(cache[device]) * device_sms(device);
   return (unsigned)std::min<uint64_t>(total, resident);
 }
-bool persistent_enabled() {
-  static const bool on = [] {
-    const char *e = std::getenv("NTT_B200_PERSISTENT");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
+bool persistent_enabled() { return tuned("ntt_persistent") != 0; }
 
 template <int LOGN, int MODE, bool INV>
 void launch_col_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
@@ -416,21 +435,29 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     }
     return;
   }
+#define NTT_LAUNCH(kernel, batch)                                                          \
+  do {                                                                                     \
+    if (tuned("ntt_minb_" #kernel) == 3)                                                   \
+      b200::ntt_##kernel<LOGN, MODE, 3><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
+    else                                                                                   \
+      b200::ntt_##kernel<LOGN, MODE, 4><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
+  } while (0)
   if (!inverse) {
     Timed t1("ntt_fwd_col", st);
-    b200::ntt_fwd_col<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
+    NTT_LAUNCH(fwd_col, b);
     t1.done();
     Timed t2("ntt_fwd_row", st);
-    b200::ntt_fwd_row<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+    NTT_LAUNCH(fwd_row, second);
     t2.done();
   } else {
     Timed t1("ntt_inv_row", st);
-    b200::ntt_inv_row<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(b, c.tables);
+    NTT_LAUNCH(inv_row, b);
     t1.done();
     Timed t2("ntt_inv_col", st);
-    b200::ntt_inv_col<LOGN, MODE><<<grid, b200::kNttThreads, 0, st>>>(second, c.tables);
+    NTT_LAUNCH(inv_col, second);
     t2.done();
   }
+#undef NTT_LAUNCH
 }
 
 template <int MODE>
@@ -531,15 +558,9 @@ std::vector<uint16_t> qp_ids(const Ctx &c, size_t level) {
 }
 
 // ---- conversion launches ---------------------------------------------------------
-// NTT_B200_CONV_LIMBS=0 selects the 128-bit-accumulator kernel for every plan
-// (the two kernels give identical results; the switch exists for measurement).
-bool conv_limbs_enabled() {
-  static const bool on = [] {
-    const char *e = std::getenv("NTT_B200_CONV_LIMBS");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
+// The "conv_limbs" tunable selects between the limb kernel and the 128-bit-
+// accumulator kernel where both apply (identical results).
+bool conv_limbs_enabled() { return tuned("conv_limbs") != 0; }
 template <int MAXS>
 void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, bool lazy_out, cudaStream_t st) {
   if constexpr (MAXS <= 8) {
@@ -576,7 +597,7 @@ void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
   // inputs y_j are then computed once per coefficient); otherwise split the
   // targets across blocks for parallelism.
   const size_t base_blocks = ((c.n + b200::kEwThreads - 1) / b200::kEwThreads) * polys;
-  const size_t want_blocks = 148 * 8;
+  const size_t want_blocks = (size_t)device_sms(c.device) * (size_t)tuned("conv_blocks_per_sm");
   int tpb = p.t;
   if (base_blocks < want_blocks) tpb = std::max<int>(4, (int)((p.t * base_blocks + want_blocks - 1) / want_blocks));
   a.targets_per_block = std::min(tpb, p.t);
@@ -983,6 +1004,27 @@ extern "C" {
 
 const char *ntt_b200_last_error(void) { return g_last_error.c_str(); }
 uint64_t ntt_b200_kernel_launches(void) { return g_launches.load(); }
+
+int ntt_b200_tuning_set(const char *name, int64_t value) {
+  return guarded([&] {
+    Tunable *t = find_tunable(name);
+    require(t != nullptr, "unknown tunable");
+    require(value >= t->lo && value <= t->hi, "tunable value out of range");
+    t->value.store(value);
+  });
+}
+
+int ntt_b200_tuning_get(const char *name, int64_t *value) {
+  return guarded([&] {
+    Tunable *t = find_tunable(name);
+    require(t != nullptr && value != nullptr, "unknown tunable");
+    *value = t->value.load();
+  });
+}
+
+const char *ntt_b200_tuning_name(size_t index) {
+  return index < sizeof(g_tuning) / sizeof(g_tuning[0]) ? g_tuning[index].name : nullptr;
+}
 
 int ntt_b200_timing_enable(int on) {
   return guarded([&] { g_timer.enabled = on != 0; });

@@ -69,9 +69,9 @@ __device__ __forceinline__ const u64 *poly_add(const NttBatch &b, u64 z) {
   return b.add_list ? b.add_list[z] : nullptr;
 }
 
-#ifndef NTT_MINB
-#define NTT_MINB 4
-#endif
+// MINB: minimum resident CTAs per SM the compiler must allow (register cap
+// 65536 / (256 * MINB)); 4 gives 32 warps per SM at 64 registers, 3 gives 24
+// warps at 85 registers. The autotuner picks it per pass.
 
 struct TowerView {
   const TowerConsts *c;
@@ -141,8 +141,8 @@ struct ColGeom {
   }
 };
 
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
+template <int LOGN, int MODE, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
   __shared__ u64 tile[kTileWords];
@@ -198,8 +198,8 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_col(NttBatch b,
   store_block<G::R, G::COLS, G::COLS, false>(v.dst + col0, tile, N >> G::LR);
 }
 
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
+template <int LOGN, int MODE, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
   __shared__ u64 tile[kTileWords];
@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_col(NttBatch b,
 // (one pad word per 16) so both mappings are bank-conflict free.
 __device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
 
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
+template <int LOGN, int MODE, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
   __shared__ u64 tile[16 * kRowPad];
   const TowerView v = tower_view(b, T, false);
@@ -336,8 +336,8 @@ __global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_fwd_row(NttBatch b,
   }
 }
 
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__(kNttThreads, NTT_MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
+template <int LOGN, int MODE, int MINB>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
   __shared__ u64 tile[16 * kRowPad];
   const TowerView v = tower_view(b, T, true);
