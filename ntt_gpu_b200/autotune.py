@@ -3,7 +3,8 @@
 Every tunable (ntt_b200_tuning_name) is a launch choice that never changes a
 result: the NTT pass variant (one CTA per tile, or persistent and double
 buffered), the register budget each NTT pass is compiled for (3 or 4 resident
-CTAs per SM), the conversion kernel (30-bit limbs or 128-bit accumulators) and
+CTAs per SM), whether the row passes stage their twiddles in shared memory, the
+conversion kernel (30-bit limbs or 128-bit accumulators) and
 the conversion grid target. The tuner runs coordinate descent over them on two
 workloads:
 
@@ -85,6 +86,8 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("ntt_minb_fwd_row", (3, 4), ntt_step, ("ntt_fwd_row",)),
         ("ntt_minb_inv_row", (3, 4), ntt_step, ("ntt_inv_row",)),
         ("ntt_minb_inv_col", (3, 4), ntt_step, ("ntt_inv_col",)),
+        ("ntt_stage_tw_fwd_row", (0, 1), ntt_step, ("ntt_fwd_row",)),
+        ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",)),
         ("conv_limbs", (0, 1), ks_step, ("conv",)),
         ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",)),
     ]

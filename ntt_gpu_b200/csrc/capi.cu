@@ -350,6 +350,8 @@ Tunable g_tuning[] = {
     {"ntt_minb_fwd_row", {4}, 3, 4},
     {"ntt_minb_inv_row", {4}, 3, 4},
     {"ntt_minb_inv_col", {4}, 3, 4},
+    {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
+    {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
 };
@@ -435,23 +437,29 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     }
     return;
   }
-#define NTT_LAUNCH(kernel, batch)                                                          \
-  do {                                                                                     \
-    if (tuned("ntt_minb_" #kernel) == 3)                                                   \
-      b200::ntt_##kernel<LOGN, MODE, 3><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
-    else                                                                                   \
-      b200::ntt_##kernel<LOGN, MODE, 4><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
+#define NTT_LAUNCH(kernel, batch, ...)                                                        \
+  do {                                                                                        \
+    if (tuned("ntt_minb_" #kernel) == 3)                                                      \
+      b200::ntt_##kernel<LOGN, MODE, 3, ##__VA_ARGS__><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
+    else                                                                                      \
+      b200::ntt_##kernel<LOGN, MODE, 4, ##__VA_ARGS__><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
   } while (0)
   if (!inverse) {
     Timed t1("ntt_fwd_col", st);
     NTT_LAUNCH(fwd_col, b);
     t1.done();
     Timed t2("ntt_fwd_row", st);
-    NTT_LAUNCH(fwd_row, second);
+    if (tuned("ntt_stage_tw_fwd_row"))
+      NTT_LAUNCH(fwd_row, second, true);
+    else
+      NTT_LAUNCH(fwd_row, second, false);
     t2.done();
   } else {
     Timed t1("ntt_inv_row", st);
-    NTT_LAUNCH(inv_row, b);
+    if (tuned("ntt_stage_tw_inv_row"))
+      NTT_LAUNCH(inv_row, b, true);
+    else
+      NTT_LAUNCH(inv_row, b, false);
     t1.done();
     Timed t2("ntt_inv_col", st);
     NTT_LAUNCH(inv_col, second);

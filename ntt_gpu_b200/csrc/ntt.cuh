@@ -108,8 +108,12 @@ __device__ __forceinline__ void load_block(u64 *smem, const u64 *g, u64 stride) 
     const int r = j / (WIDTH / 2), c = (j % (WIDTH / 2)) * 2;
     const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(g + r * stride + c);
     const int s = r * PITCH + c + (PAD16 ? (c >> 4) : 0);
-    smem[s] = v.x;
-    smem[s + 1] = v.y;
+    if constexpr (PAD16) {  // padded rows: s may be odd, so two 8-byte stores
+      smem[s] = v.x;
+      smem[s + 1] = v.y;
+    } else {  // one 16-byte store (no bank conflict)
+      *reinterpret_cast<ulonglong2 *>(smem + s) = v;
+    }
   }
 }
 template <int ROWS, int WIDTH, int PITCH, bool PAD16>
@@ -119,8 +123,12 @@ __device__ __forceinline__ void store_block(u64 *g, const u64 *smem, u64 stride)
     const int r = j / (WIDTH / 2), c = (j % (WIDTH / 2)) * 2;
     const int s = r * PITCH + c + (PAD16 ? (c >> 4) : 0);
     ulonglong2 v;
-    v.x = smem[s];
-    v.y = smem[s + 1];
+    if constexpr (PAD16) {
+      v.x = smem[s];
+      v.y = smem[s + 1];
+    } else {
+      v = *reinterpret_cast<const ulonglong2 *>(smem + s);
+    }
     *reinterpret_cast<ulonglong2 *>(g + r * stride + c) = v;
   }
 }
@@ -145,7 +153,7 @@ template <int LOGN, int MODE, int MINB>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
-  __shared__ u64 tile[kTileWords];
+  __shared__ __align__(16) u64 tile[kTileWords];
   __shared__ ulonglong2 tw[G::R];
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
@@ -202,7 +210,7 @@ template <int LOGN, int MODE, int MINB>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
-  __shared__ u64 tile[kTileWords];
+  __shared__ __align__(16) u64 tile[kTileWords];
   __shared__ ulonglong2 tw[G::R];
   const TowerView v = tower_view(b, T, true);
   const u64 q = v.c->q, q2 = v.c->q2;
@@ -261,10 +269,28 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
 // (one pad word per 16) so both mappings are bank-conflict free.
 __device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
 
-template <int LOGN, int MODE, int MINB>
+// Twiddle staging for the row passes' register-bit stages (s' = 4..7, where
+// lane u of row r needs T[2^s + (row << s') + ((16u + e) >> (8 - s'))]): with STW
+// set, the CTA first copies the stage's 16 * 2^s' twiddles, contiguous in the
+// table, into shared memory with coalesced 16-byte loads, entry k at 16-byte
+// slot k + k/8. The pad keeps the eight lanes of every quarter-warp on distinct
+// bank groups for all four stages, and the data tile's buffer (free while the
+// values sit in registers) holds the largest stage (2048 entries, 36 KiB).
+constexpr int kRowStwWords = 2 * (2048 + 2048 / 8);
+__device__ __forceinline__ void stage_twiddles(ulonglong2 *st, const ulonglong2 *tw, int s, int sp, int row0) {
+  const ulonglong2 *src = tw + (1 << s) + (row0 << sp);
+  const int count = 16 << sp;
+  for (int k = threadIdx.x; k < count; k += kNttThreads) st[k + (k >> 3)] = __ldg(src + k);
+}
+__device__ __forceinline__ Shoup staged_twiddle(const ulonglong2 *st, int k) {
+  const ulonglong2 v = st[k + (k >> 3)];
+  return Shoup{v.x, v.y};
+}
+
+template <int LOGN, int MODE, int MINB, bool STW>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
-  __shared__ u64 tile[16 * kRowPad];
+  __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
@@ -294,14 +320,32 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
 #pragma unroll
   for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
   // Stages LR + s', s' = 4..7: column bit 7-s' == register bit 7-s'.
+  if constexpr (STW) {
+    ulonglong2 *st = reinterpret_cast<ulonglong2 *>(tile);
 #pragma unroll
-  for (int sp = 4; sp < 8; ++sp) {
-    const int s = LR + sp, d = 1 << (7 - sp);
+    for (int sp = 4; sp < 8; ++sp) {
+      const int s = LR + sp, d = 1 << (7 - sp);
+      __syncthreads();  // the tile (data, or the previous stage's twiddles) is no longer read
+      stage_twiddles(st, v.tw, s, sp, row0);
+      __syncthreads();
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      if (e & d) continue;
-      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
-      ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const Shoup w = staged_twiddle(st, (r << sp) + ((u * 16 + e) >> (8 - sp)));
+        ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
+    }
+    __syncthreads();  // staged twiddles read by every warp before the data returns
+  } else {
+#pragma unroll
+    for (int sp = 4; sp < 8; ++sp) {
+      const int s = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+        ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
     }
   }
 #pragma unroll
@@ -336,10 +380,10 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   }
 }
 
-template <int LOGN, int MODE, int MINB>
+template <int LOGN, int MODE, int MINB, bool STW>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
   constexpr int LR = LOGN - 8;
-  __shared__ u64 tile[16 * kRowPad];
+  __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
   const TowerView v = tower_view(b, T, true);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
@@ -352,14 +396,32 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
 #pragma unroll
   for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
   // Stages LR + s', s' = 7..4: column bit 7-s' == register bit 7-s'.
+  if constexpr (STW) {
+    ulonglong2 *st = reinterpret_cast<ulonglong2 *>(tile);
 #pragma unroll
-  for (int sp = 7; sp >= 4; --sp) {
-    const int s = LR + sp, d = 1 << (7 - sp);
+    for (int sp = 7; sp >= 4; --sp) {
+      const int s = LR + sp, d = 1 << (7 - sp);
+      __syncthreads();  // the tile (data, or the previous stage's twiddles) is no longer read
+      stage_twiddles(st, v.tw, s, sp, row0);
+      __syncthreads();
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      if (e & d) continue;
-      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
-      gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const Shoup w = staged_twiddle(st, (r << sp) + ((u * 16 + e) >> (8 - sp)));
+        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
+    }
+    __syncthreads();  // staged twiddles read by every warp before the data returns
+  } else {
+#pragma unroll
+    for (int sp = 7; sp >= 4; --sp) {
+      const int s = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
     }
   }
   __syncwarp();
