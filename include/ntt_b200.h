@@ -67,6 +67,9 @@ int ntt_b200_context_table_bytes(ntt_b200_context ctx, size_t *out);
 /* Build every conversion/correction plan a key switch at `level` needs, so that
  * later calls at that level perform no host work or table upload. */
 int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level);
+/* Words of one channel of a full-context switching key: digits x (M + K) x N
+ * (the packing of Session::upload_hybrid_key's source, src/resident.cpp:492-529). */
+int ntt_b200_context_key_words(ntt_b200_context ctx, size_t *words);
 
 /* Forward (inverse = 0) or inverse NTT of `polys` polynomials. Slot i of poly p
  * is read at src + p*poly_stride + i*N and written at dst + p*poly_stride + i*N
@@ -181,6 +184,9 @@ typedef struct ntt_b200_ks_request {
   const uint64_t *add_a;
   uint32_t automorphism;
   uint32_t level;
+  /* Server only: with key_b == key_a == NULL, the key is taken from the
+   * server's key cache under this id (ntt_b200_server_attach_keycache). */
+  uint64_t key_id;
 } ntt_b200_ks_request;
 
 /* Workspace bytes of ntt_b200_keyswitch_requests for this request list. */
@@ -195,6 +201,37 @@ int ntt_b200_keyswitch_requests_workspace(ntt_b200_context ctx, const ntt_b200_k
  * (src/resident.cpp:458-617) and run_hybrid_core. */
 int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request *reqs, size_t count,
                                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* Evaluation-key cache. Keys live in pinned host memory owned by the cache
+ * (copied at insert) and are made resident in HBM on demand within a byte
+ * budget. acquire() uploads on the caller's stream if needed (stream-ordered),
+ * evicting least-recently-used keys that are unpinned and whose last release
+ * has completed on the GPU, pins the key and returns its device pointers;
+ * release() unpins it in stream order (the key stays in place until the work
+ * enqueued before the release has completed). set_budget() evicts eligible keys
+ * first and refuses a budget that pinned keys prevent; trim() evicts every
+ * eligible key. This is the evaluation-key cache the reference proposes but does
+ * not implement (include/ntt/backend_api.hpp:51-79 CacheStats /
+ * set_cache_budget / trim_cache; include/ntt/backend_contract.hpp:322-352
+ * EvaluationKeyCacheKey, here a caller-chosen 64-bit id). */
+typedef struct ntt_b200_keycache_s *ntt_b200_keycache;
+typedef struct ntt_b200_keycache_report {
+  size_t budget_bytes, allocated_bytes, pinned_bytes;
+  uint64_t keys, resident, hits, misses, evictions;
+} ntt_b200_keycache_report;
+const char *ntt_b200_keycache_last_error(void);
+int ntt_b200_keycache_create(ntt_b200_keycache *out, int device, size_t budget_bytes);
+int ntt_b200_keycache_destroy(ntt_b200_keycache cache);
+/* Host key_b / key_a: full-context digits of ntt_b200_context_key_words each. */
+int ntt_b200_keycache_insert(ntt_b200_keycache cache, ntt_b200_context ctx, uint64_t key_id,
+                             const uint64_t *host_b, const uint64_t *host_a);
+int ntt_b200_keycache_contains(ntt_b200_keycache cache, uint64_t key_id, ntt_b200_context *ctx);
+int ntt_b200_keycache_acquire(ntt_b200_keycache cache, uint64_t key_id, void *stream,
+                              const uint64_t **key_b, const uint64_t **key_a);
+int ntt_b200_keycache_release(ntt_b200_keycache cache, uint64_t key_id, void *stream);
+int ntt_b200_keycache_stats(ntt_b200_keycache cache, ntt_b200_keycache_report *out);
+int ntt_b200_keycache_set_budget(ntt_b200_keycache cache, size_t bytes);
+int ntt_b200_keycache_trim(ntt_b200_keycache cache, size_t *freed);
 
 /* Continuous-batching key-switch server. Requests (ntt_b200_ks_request: key
  * switch, relinearization or rotation) arrive from any host thread and refer to
@@ -246,6 +283,12 @@ int ntt_b200_server_drain(ntt_b200_server srv, uint32_t timeout_ms);
 int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int reset);
 /* Finishes pending and in-flight work, then frees the server. */
 int ntt_b200_server_destroy(ntt_b200_server srv);
+/* Requests submitted with key_b == key_a == NULL take their key from `cache`
+ * by key_id: each wave acquires its keys on its lane's stream at launch and
+ * releases them in stream order after it. A wave whose keys do not fit the
+ * cache's budget next to the keys of the waves in flight waits for them. The
+ * cache must outlive the server. */
+int ntt_b200_server_attach_keycache(ntt_b200_server srv, ntt_b200_keycache cache);
 
 /* MAC with per-digit device pointers (count digits of L+K towers each):
  * full_key_rows != 0 -> key pointers are full-context digits (rows chosen by

@@ -17,7 +17,7 @@ import os
 
 from .build import LIB
 
-__all__ = ["ContractError", "CudaError", "WorkspaceError", "Context", "KsRequest", "make_request", "Server",
+__all__ = ["ContractError", "CudaError", "WorkspaceError", "Context", "KsRequest", "make_request", "Server", "KeyCache",
            "library", "load",
            "kernel_launches", "OP_MOD_UP", "OP_MOD_DOWN", "OP_DIGITS", "OP_KEYSWITCH"]
 
@@ -73,6 +73,18 @@ _SIGNATURES = {
     "ntt_b200_server_drain": ([_P, ctypes.c_uint32], _I),
     "ntt_b200_server_stats": ([_P, _P, _I], _I),
     "ntt_b200_server_destroy": ([_P], _I),
+    "ntt_b200_server_attach_keycache": ([_P, _P], _I),
+    "ntt_b200_context_key_words": ([_P, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_keycache_last_error": ([], ctypes.c_char_p),
+    "ntt_b200_keycache_create": ([ctypes.POINTER(_P), _I, _SZ], _I),
+    "ntt_b200_keycache_destroy": ([_P], _I),
+    "ntt_b200_keycache_insert": ([_P, _P, _U64, _P, _P], _I),
+    "ntt_b200_keycache_contains": ([_P, _U64, ctypes.POINTER(_P)], _I),
+    "ntt_b200_keycache_acquire": ([_P, _U64, _P, ctypes.POINTER(_P), ctypes.POINTER(_P)], _I),
+    "ntt_b200_keycache_release": ([_P, _U64, _P], _I),
+    "ntt_b200_keycache_stats": ([_P, _P], _I),
+    "ntt_b200_keycache_set_budget": ([_P, _SZ], _I),
+    "ntt_b200_keycache_trim": ([_P, ctypes.POINTER(_SZ)], _I),
     "ntt_b200_stream_create": ([_I, ctypes.POINTER(_P)], _I),
     "ntt_b200_stream_destroy": ([_P], _I),
     "ntt_b200_stream_synchronize": ([_P], _I),
@@ -98,7 +110,8 @@ _SIGNATURES = {
 class KsRequest(ctypes.Structure):
     """ntt_b200_ks_request: one key-switch / rotation / relinearization request."""
     _fields_ = [("src", _P), ("out_b", _P), ("out_a", _P), ("key_b", _P), ("key_a", _P), ("c0", _P),
-                ("add_b", _P), ("add_a", _P), ("automorphism", ctypes.c_uint32), ("level", ctypes.c_uint32)]
+                ("add_b", _P), ("add_a", _P), ("automorphism", ctypes.c_uint32), ("level", ctypes.c_uint32),
+                ("key_id", _U64)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -116,10 +129,17 @@ class ServerReport(ctypes.Structure):
                 ("mean_queue_ms", ctypes.c_double), ("peak_bytes", _SZ), ("in_flight_bytes", _SZ)]
 
 
-def make_request(level, src, out_b, out_a, key_b, key_a, c0=None, automorphism=0, add_b=None, add_a=None):
-    """A KsRequest from torch CUDA tensors (None for the optional ones)."""
+def make_request(level, src, out_b, out_a, key_b=None, key_a=None, c0=None, automorphism=0, add_b=None, add_a=None,
+                 key_id=0):
+    """A KsRequest from torch CUDA tensors (None for the optional ones). With
+    key_b = key_a = None the server takes the key from its key cache by key_id."""
     return KsRequest(_ptr(src), _ptr(out_b), _ptr(out_a), _ptr(key_b), _ptr(key_a), _ptr(c0), _ptr(add_b),
-                     _ptr(add_a), int(automorphism), int(level))
+                     _ptr(add_a), int(automorphism), int(level), int(key_id))
+
+
+class KeyCacheReport(ctypes.Structure):
+    _fields_ = [("budget_bytes", _SZ), ("allocated_bytes", _SZ), ("pinned_bytes", _SZ), ("keys", _U64),
+                ("resident", _U64), ("hits", _U64), ("misses", _U64), ("evictions", _U64)]
 
 
 TUNING = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
@@ -175,11 +195,12 @@ def kernel_launches() -> int:
     return int(load().ntt_b200_kernel_launches())
 
 
-def _check(rc: int, server: bool = False):
+def _check(rc: int, server: bool = False, cache: bool = False):
     if rc == OK:
         return
     lib = load()
-    msg = (lib.ntt_b200_server_last_error() if server else lib.ntt_b200_last_error()).decode()
+    msg = (lib.ntt_b200_server_last_error() if server else
+           lib.ntt_b200_keycache_last_error() if cache else lib.ntt_b200_last_error()).decode()
     if rc == ERR_CONTRACT or rc == ERR_UNSUPPORTED:
         raise ContractError(msg)
     if rc == ERR_WORKSPACE:
@@ -361,6 +382,10 @@ class Server:
         _check(self._lib.ntt_b200_server_wait(self._h, ticket, timeout_ms, ctypes.byref(info)), server=True)
         return info
 
+    def attach_keycache(self, cache: "KeyCache"):
+        _check(self._lib.ntt_b200_server_attach_keycache(self._h, cache._h), server=True)
+        self._cache = cache  # the cache outlives the server
+
     def drain(self, timeout_ms: int = 120000):
         _check(self._lib.ntt_b200_server_drain(self._h, timeout_ms), server=True)
 
@@ -372,6 +397,64 @@ class Server:
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             _check(self._lib.ntt_b200_server_destroy(self._h), server=True)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class KeyCache:
+    """Evaluation-key cache (ntt_b200_keycache_*): host keys made resident in
+    HBM on demand within a byte budget, least-recently-used eviction of keys
+    that are unpinned and whose last use has completed."""
+
+    def __init__(self, device=0, budget_bytes=8 << 30):
+        self._lib = load()
+        h = _P()
+        _check(self._lib.ntt_b200_keycache_create(ctypes.byref(h), int(device), int(budget_bytes)), cache=True)
+        self._h = h
+
+    def insert(self, ctx: "Context", key_id: int, key_b, key_a):
+        """key_b / key_a: host numpy uint64 arrays of full-context digits."""
+        import numpy as np
+        kb = np.ascontiguousarray(key_b, dtype=np.uint64)
+        ka = np.ascontiguousarray(key_a, dtype=np.uint64)
+        words = _SZ()
+        _check(self._lib.ntt_b200_context_key_words(ctx._h, ctypes.byref(words)))
+        if kb.size != words.value or ka.size != words.value:
+            raise ContractError(f"key must hold {words.value} words per channel")
+        _check(self._lib.ntt_b200_keycache_insert(self._h, ctx._h, int(key_id), kb.ctypes.data, ka.ctypes.data),
+               cache=True)
+
+    def acquire(self, key_id: int, stream=None):
+        """(key_b, key_a) device addresses, pinned until release()."""
+        b, a = _P(), _P()
+        _check(self._lib.ntt_b200_keycache_acquire(self._h, int(key_id), _stream(stream), ctypes.byref(b),
+                                                   ctypes.byref(a)), cache=True)
+        return b.value, a.value
+
+    def release(self, key_id: int, stream=None):
+        _check(self._lib.ntt_b200_keycache_release(self._h, int(key_id), _stream(stream)), cache=True)
+
+    def stats(self) -> dict:
+        st = KeyCacheReport()
+        _check(self._lib.ntt_b200_keycache_stats(self._h, ctypes.byref(st)), cache=True)
+        return {f: getattr(st, f) for f, _ in KeyCacheReport._fields_}
+
+    def set_budget(self, nbytes: int):
+        _check(self._lib.ntt_b200_keycache_set_budget(self._h, int(nbytes)), cache=True)
+
+    def trim(self) -> int:
+        freed = _SZ()
+        _check(self._lib.ntt_b200_keycache_trim(self._h, ctypes.byref(freed)), cache=True)
+        return freed.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(self._lib.ntt_b200_keycache_destroy(self._h), cache=True)
             self._h = _P()
 
     def __del__(self):

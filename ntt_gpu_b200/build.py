@@ -1,7 +1,7 @@
 """Build recipe for the in-tree sm_100a library (libntt_b200.so).
 
-Compiles ntt_gpu_b200/csrc/capi.cu (which includes every kernel header) and
-server.cpp with nvcc for sm_100a only and writes ntt_gpu_b200/lib/libntt_b200.so. The library
+Compiles ntt_gpu_b200/csrc/capi.cu (which includes every kernel header),
+server.cpp and keycache.cpp with nvcc for sm_100a only and writes ntt_gpu_b200/lib/libntt_b200.so. The library
 travels with the source tree; nothing is installed into site-packages.
 """
 from __future__ import annotations
@@ -69,7 +69,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(LIB, sources() + [header, __file__]):
         nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
         tmp = LIB + ".tmp"
-        cmd = [nvcc, *NVCC_FLAGS, "-o", tmp, os.path.join(CSRC, "capi.cu"), os.path.join(CSRC, "server.cpp")]
+        cmd = [nvcc, *NVCC_FLAGS, "-o", tmp, os.path.join(CSRC, "capi.cu"), os.path.join(CSRC, "server.cpp"),
+               os.path.join(CSRC, "keycache.cpp")]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -1156,6 +1156,14 @@ int ntt_b200_context_table_bytes(ntt_b200_context ctx, size_t *out) {
   });
 }
 
+int ntt_b200_context_key_words(ntt_b200_context ctx, size_t *words) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(words != nullptr, "null output");
+    *words = (1 + (ctx->m - 1) / ctx->alpha) * ctx->towers() * ctx->n;
+  });
+}
+
 int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level) {
   return guarded([&] {
     require_ctx(ctx);

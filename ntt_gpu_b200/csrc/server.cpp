@@ -81,6 +81,7 @@ struct ntt_b200_server_s {
   std::vector<Lane> lanes;
   std::vector<std::unique_ptr<Wave>> waves_in_flight;
   std::vector<cudaEvent_t> event_pool;
+  ntt_b200_keycache keycache = nullptr;  // resolves requests submitted by key id
   int depth = 1;
   uint64_t next_id = 1;
   size_t in_use = 0, peak_in_use = 0;
@@ -219,6 +220,35 @@ struct ntt_b200_server_s {
       reqs.resize(keep);
       wave.resize(keep);
     }
+    // Keys by id: acquire them on the lane's stream (uploading what is not
+    // resident); they are released in stream order right after the wave.
+    // A wave whose keys do not all fit the cache's budget is cut to the
+    // requests whose keys were acquired; the rest stay pending.
+    std::vector<uint64_t> acquired;
+    if (keycache) {
+      for (size_t i = 0; i < reqs.size(); ++i) {
+        auto &r = reqs[i];
+        if (r.key_b || r.key_a) continue;
+        const uint64_t *kb = nullptr, *ka = nullptr;
+        const int krc = ntt_b200_keycache_acquire(keycache, r.key_id, lanes[lane].stream, &kb, &ka);
+        if (krc == NTT_B200_ERR_WORKSPACE && i > 0) {
+          reqs.resize(i);
+          wave.resize(i);
+          break;
+        }
+        if (krc != NTT_B200_OK) {
+          const std::string why = ntt_b200_keycache_last_error();
+          for (uint64_t id : acquired) ntt_b200_keycache_release(keycache, id, lanes[lane].stream);
+          if (krc == NTT_B200_ERR_WORKSPACE && any_busy()) return false;  // wait for in-flight keys
+          fail_ticket(wave[0], krc, why);
+          erase_pending({wave[0]});
+          return true;
+        }
+        acquired.push_back(r.key_id);
+        r.key_b = kb;
+        r.key_a = ka;
+      }
+    }
     // Reserve the lane and the memory, then launch without the lock.
     erase_pending(wave);
     const double t_launch = now_us();
@@ -266,9 +296,11 @@ struct ntt_b200_server_s {
     if (e != cudaSuccess) {
       rc = NTT_B200_ERR_CUDA;
       why = std::string("CUDA: lane arena: ") + cudaGetErrorString(e);
+      for (uint64_t id : acquired) ntt_b200_keycache_release(keycache, id, stream);
     } else {
       rc = ntt_b200_keyswitch_requests(ctx, reqs.data(), reqs.size(), ws, ws_bytes, stream);
       if (rc != NTT_B200_OK) why = ntt_b200_last_error();
+      for (uint64_t id : acquired) ntt_b200_keycache_release(keycache, id, stream);
       if (rc == NTT_B200_OK) {
         e = cudaEventRecord(done, stream);
         if (e != cudaSuccess) {
@@ -375,8 +407,23 @@ int ntt_b200_server_submit(ntt_b200_server srv, ntt_b200_context ctx, const ntt_
     if (!srv || !ctx || !req || !ticket) return contract("null argument");
     // Validate the request alone before it joins a wave: a bad request is
     // refused here and never fails the requests it would have been batched with.
+    ntt_b200_ks_request check = *req;
+    if (!req->key_b && !req->key_a) {
+      ntt_b200_context owner = nullptr;
+      ntt_b200_keycache cache = nullptr;
+      {
+        std::lock_guard<std::mutex> lock(srv->mu);
+        cache = srv->keycache;
+      }
+      if (!cache) return contract("request without key pointers, and no key cache attached");
+      if (ntt_b200_keycache_contains(cache, req->key_id, &owner) != NTT_B200_OK || owner != ctx)
+        return contract("key id not in the attached key cache for this context");
+      // Placeholder key addresses for the host-side checks (sizes, alignment,
+      // overlap): far below any device allocation, never dereferenced.
+      check.key_b = check.key_a = reinterpret_cast<const uint64_t *>(uintptr_t(256));
+    }
     size_t need = 0;
-    if (ntt_b200_keyswitch_requests_workspace(ctx, req, 1, &need) != NTT_B200_OK) {
+    if (ntt_b200_keyswitch_requests_workspace(ctx, &check, 1, &need) != NTT_B200_OK) {
       g_server_error = ntt_b200_last_error();
       return NTT_B200_ERR_CONTRACT;
     }
@@ -478,6 +525,15 @@ int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int 
       srv->first_submit = srv->last_done = srv->queue_us = 0;
       srv->peak_in_use = srv->in_use;
     }
+    return NTT_B200_OK;
+  });
+}
+
+int ntt_b200_server_attach_keycache(ntt_b200_server srv, ntt_b200_keycache cache) {
+  return server_guard([&] {
+    if (!srv) return contract("null server");
+    std::lock_guard<std::mutex> lock(srv->mu);
+    srv->keycache = cache;
     return NTT_B200_OK;
   });
 }
