@@ -55,14 +55,17 @@ def test_cache_lru_pins_budget_and_exact_keys(lib, orc):
     # 0 miss, 1 miss, 0 hit, 2 miss (evicts 1), 3 miss (evicts 0), 1 miss (evicts 2)
     assert (st["hits"], st["misses"], st["evictions"]) == (1, 5, 3)
     assert st["resident"] == 2 and st["allocated_bytes"] == 2 * key_bytes <= st["budget_bytes"]
-    # A pinned key blocks a budget below it; after release it can be trimmed away.
+    # A pinned key blocks a budget below it. The refused call still evicts the
+    # eligible key 1 first (evict eligible entries, then reject); after its
+    # release, key 3 is trimmed away.
     cache.acquire(3)
     with pytest.raises(nb.ContractError):
         cache.set_budget(key_bytes // 2)
+    assert cache.stats()["evictions"] == 4 and cache.stats()["pinned_bytes"] == key_bytes
     import torch
     cache.release(3)
     torch.cuda.synchronize()
-    assert cache.trim() == 2 * key_bytes
+    assert cache.trim() == key_bytes
     cache.set_budget(key_bytes)
     assert cache.stats()["allocated_bytes"] == 0
     with pytest.raises(nb.ContractError):
