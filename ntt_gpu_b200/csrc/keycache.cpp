@@ -28,6 +28,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/ntt_b200.h"
 
@@ -84,9 +85,11 @@ struct ntt_b200_keycache_s {
   // Evict least-recently-used eligible entries until `need` more bytes fit
   // under `limit` (lock held).
   int make_room(size_t need, size_t limit) {
-    for (auto it = lru.rbegin(); it != lru.rend() && allocated + need > limit;) {
-      const uint64_t id = *it;
-      ++it;  // evict() erases the element the iterator referred to
+    // Snapshot the resident ids, least recently used first: evict() erases list
+    // nodes, so the list itself is not walked while evicting.
+    const std::vector<uint64_t> order(lru.rbegin(), lru.rend());
+    for (uint64_t id : order) {
+      if (allocated + need <= limit) break;
       Entry &e = entries.at(id);
       if (!eligible(e)) continue;
       const int rc = evict(id, e);
@@ -243,9 +246,8 @@ int ntt_b200_keycache_trim(ntt_b200_keycache c, size_t *freed) {
   if (!c) return fail(NTT_B200_ERR_CONTRACT, "null key cache");
   std::lock_guard<std::mutex> lock(c->mu);
   const size_t before = c->allocated;
-  for (auto it = c->lru.begin(); it != c->lru.end();) {
-    const uint64_t id = *it;
-    ++it;
+  const std::vector<uint64_t> order(c->lru.begin(), c->lru.end());
+  for (uint64_t id : order) {
     Entry &e = c->entries.at(id);
     if (c->eligible(e)) {
       const int rc = c->evict(id, e);

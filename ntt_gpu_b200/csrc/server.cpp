@@ -459,12 +459,13 @@ int ntt_b200_server_wait(ntt_b200_server srv, uint64_t ticket, uint32_t timeout_
     if (it == srv->tickets.end()) return contract("unknown or already collected ticket");
     const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
     while (it->second.status == NTT_B200_NOT_READY) {
-      if (srv->cv_done.wait_until(lock, deadline) == std::cv_status::timeout &&
-          srv->tickets.find(ticket)->second.status == NTT_B200_NOT_READY) {
+      const bool timed_out = srv->cv_done.wait_until(lock, deadline) == std::cv_status::timeout;
+      it = srv->tickets.find(ticket);
+      if (it == srv->tickets.end()) return contract("ticket collected by another waiter");
+      if (timed_out && it->second.status == NTT_B200_NOT_READY) {
         g_server_error = "ticket not complete within the timeout";
         return NTT_B200_ERR_TIMEOUT;
       }
-      it = srv->tickets.find(ticket);
     }
     const Ticket &t = it->second;
     if (info) {
