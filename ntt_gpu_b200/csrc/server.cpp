@@ -45,6 +45,11 @@ double now_us() {
   return duration<double, std::micro>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Placeholder key address for the host-side checks (sizes, alignment, overlap)
+// of requests that name their key by id: far below any device allocation and
+// never dereferenced; the real pointers come from the key cache at launch.
+const uint64_t *const kKeyPlaceholder = reinterpret_cast<const uint64_t *>(uintptr_t(256));
+
 struct Ticket {
   ntt_b200_context ctx = nullptr;
   ntt_b200_ks_request req{};
@@ -186,7 +191,12 @@ struct ntt_b200_server_s {
     size_t need = 0;
     std::vector<int> release;  // idle lanes whose arenas this wave takes over
     while (true) {
-      if (ntt_b200_keyswitch_requests_workspace(ctx, reqs.data(), reqs.size(), &need) != NTT_B200_OK) {
+      // Requests by key id carry no key pointers yet: size them with the
+      // placeholder addresses used at submission.
+      std::vector<ntt_b200_ks_request> sized(reqs);
+      for (auto &r : sized)
+        if (!r.key_b && !r.key_a) r.key_b = r.key_a = kKeyPlaceholder;
+      if (ntt_b200_keyswitch_requests_workspace(ctx, sized.data(), sized.size(), &need) != NTT_B200_OK) {
         // Requests are validated at submission; a failure here fails the wave.
         const std::string why = ntt_b200_last_error();
         for (uint64_t id : wave) fail_ticket(id, NTT_B200_ERR_CONTRACT, why);
@@ -418,9 +428,7 @@ int ntt_b200_server_submit(ntt_b200_server srv, ntt_b200_context ctx, const ntt_
       if (!cache) return contract("request without key pointers, and no key cache attached");
       if (ntt_b200_keycache_contains(cache, req->key_id, &owner) != NTT_B200_OK || owner != ctx)
         return contract("key id not in the attached key cache for this context");
-      // Placeholder key addresses for the host-side checks (sizes, alignment,
-      // overlap): far below any device allocation, never dereferenced.
-      check.key_b = check.key_a = reinterpret_cast<const uint64_t *>(uintptr_t(256));
+      check.key_b = check.key_a = kKeyPlaceholder;
     }
     size_t need = 0;
     if (ntt_b200_keyswitch_requests_workspace(ctx, &check, 1, &need) != NTT_B200_OK) {
