@@ -290,6 +290,27 @@ int ntt_b200_server_destroy(ntt_b200_server srv);
  * cache must outlive the server. */
 int ntt_b200_server_attach_keycache(ntt_b200_server srv, ntt_b200_keycache cache);
 
+/* Host-buffer key switch with overlapped copies. `batch` components at one
+ * level from host memory h_src[batch][L][N] into host h_out_b / h_out_a, keys
+ * (and the workspace) on the device, optional host h_c0 for rotation. The batch
+ * runs in chunks of `chunk` requests through two device staging slots: the copy
+ * to the device of one chunk, the key switch of the previous one and the copy
+ * back of the one before run concurrently on two internal copy streams and the
+ * caller's stream, so the copies in both directions overlap each other and the
+ * kernels. The call is stream-ordered: it starts after the work already on
+ * `stream`, and work enqueued after it sees every output on the host. Host
+ * buffers should be pinned (cudaHostAlloc) for the copies to overlap. Calls on
+ * one context serialise their use of its copy streams. This is the
+ * host-vector form of the reference's CudaNttTransform / synchronous Session
+ * entry points (include/ntt/cuda_ntt.hpp:34-79) for the key switch, which the
+ * reference runs as pageable copies around each call. */
+int ntt_b200_keyswitch_host_workspace(ntt_b200_context ctx, size_t level, size_t chunk, int rotate,
+                                      size_t *bytes);
+int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk,
+                            const uint64_t *h_src, uint64_t *h_out_b, uint64_t *h_out_a,
+                            const uint64_t *key_b, const uint64_t *key_a, const uint64_t *h_c0,
+                            uint32_t automorphism, void *workspace, size_t workspace_bytes, void *stream);
+
 /* MAC with per-digit device pointers (count digits of L+K towers each):
  * full_key_rows != 0 -> key pointers are full-context digits (rows chosen by
  * key_indices); 0 -> keys are already packed active QP rows. accumulate != 0

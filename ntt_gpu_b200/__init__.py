@@ -66,6 +66,8 @@ _SIGNATURES = {
     "ntt_b200_hybrid_mac_digits": ([_P, _SZ, _P, _P, _P, _P, _P, _SZ, _I, _I, _P], _I),
     "ntt_b200_keyswitch_requests_workspace": ([_P, _P, _SZ, ctypes.POINTER(_SZ)], _I),
     "ntt_b200_keyswitch_requests": ([_P, _P, _SZ, _P, _SZ, _P], _I),
+    "ntt_b200_keyswitch_host_workspace": ([_P, _SZ, _SZ, _I, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_keyswitch_host": ([_P, _SZ, _SZ, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
     "ntt_b200_server_last_error": ([], ctypes.c_char_p),
     "ntt_b200_server_create": ([ctypes.POINTER(_P), _P], _I),
     "ntt_b200_server_submit": ([_P, _P, _P, ctypes.POINTER(_U64)], _I),
@@ -349,6 +351,24 @@ class Context:
         arr = (KsRequest * len(reqs))(*reqs)
         _check(self._lib.ntt_b200_keyswitch_requests(self._h, arr, len(reqs), _ptr(workspace),
                                                      workspace.numel() * 8, _stream(stream)))
+
+    def host_workspace(self, level, chunk, rotate=False):
+        import torch
+        out = _SZ()
+        _check(self._lib.ntt_b200_keyswitch_host_workspace(self._h, level, chunk, int(rotate), ctypes.byref(out)))
+        return torch.empty(max(1, (out.value + 7) // 8), dtype=torch.int64, device=f"cuda:{self.device}")
+
+    def keyswitch_host(self, level, batch, chunk, h_src, h_out_b, h_out_a, key_b, key_a, workspace, h_c0=None,
+                       automorphism=0, stream=None):
+        """Host tensors (pinned CPU int64) in and out; keys and workspace on the device."""
+        def hp(t):
+            if t is None:
+                return None
+            assert not t.is_cuda and t.is_contiguous()
+            return t.data_ptr()
+        _check(self._lib.ntt_b200_keyswitch_host(self._h, level, batch, chunk, hp(h_src), hp(h_out_b), hp(h_out_a),
+                                                 _ptr(key_b), _ptr(key_a), hp(h_c0), automorphism, _ptr(workspace),
+                                                 workspace.numel() * 8, _stream(stream)))
 
     def keyswitch(self, level, out_b, out_a, src, key_b, key_a, workspace, c0=None, automorphism=0,
                   stream=None):

@@ -156,6 +156,13 @@ struct ntt_b200_context_s {
   std::mutex mu;
   std::map<std::pair<std::vector<uint16_t>, std::vector<uint16_t>>, HostConvPlan> conv;
   std::map<size_t, b200::DownPlan *> down;
+  // Host-buffer pipeline (ntt_b200_keyswitch_host): two copy streams and the
+  // per-slot events that hand the two device staging slots between them and
+  // the compute stream. Created on first use.
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+  cudaEvent_t ev_start = nullptr;
+  std::mutex pipe_mu;
 
   size_t towers() const { return m + k; }
 
@@ -165,6 +172,10 @@ struct ntt_b200_context_s {
     // quiescence, src/cuda/resident_adapter.inc:107-115).
     for (auto &kv : conv) cudaFree(kv.second.device);
     for (auto &kv : down) cudaFree(kv.second);
+    if (copy_in) cudaStreamDestroy(copy_in);
+    if (copy_out) cudaStreamDestroy(copy_out);
+    for (cudaEvent_t e : {ev_in[0], ev_in[1], ev_comp[0], ev_comp[1], ev_out[0], ev_out[1], ev_start})
+      if (e) cudaEventDestroy(e);
     cudaFree(d_tc);
     cudaFree(d_fwd);
     cudaFree(d_inv);
@@ -1432,6 +1443,96 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
       Carver ws{reinterpret_cast<char *>(workspace), workspace_bytes};
       run_chunk(c, reqs, ch, ws, st);
     }
+  });
+}
+
+// ---- host-buffer key switch with overlapped copies ------------------------------------
+size_t host_slot_words(const Ctx &c, size_t level, size_t chunk, bool rotate) {
+  return chunk * level * c.n * (rotate ? 4 : 3);  // src (+ c0) in, out_b + out_a
+}
+
+int ntt_b200_keyswitch_host_workspace(ntt_b200_context ctx, size_t level, size_t chunk, int rotate,
+                                      size_t *bytes) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    require(bytes != nullptr && chunk >= 1 && chunk <= 65535 / 2, "invalid host pipeline query");
+    *bytes = 2 * aligned_bytes(host_slot_words(*ctx, level, chunk, rotate != 0)) +
+             workspace_bytes(*ctx, NTT_B200_OP_KEYSWITCH, level, chunk);
+  });
+}
+
+int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk, const uint64_t *h_src,
+                            uint64_t *h_out_b, uint64_t *h_out_a, const uint64_t *key_b, const uint64_t *key_a,
+                            const uint64_t *h_c0, uint32_t automorphism, void *workspace, size_t ws_size,
+                            void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_level(ctx, level);
+    Ctx &c = *ctx;
+    require(batch >= 1 && chunk >= 1 && chunk <= 65535 / 2, "invalid batch or chunk");
+    require(h_src && h_out_b && h_out_a && key_b && key_a, "null pointer");
+    require_aligned({key_b, key_a, workspace});
+    const bool rotate = h_c0 != nullptr;
+    if (rotate) require((automorphism & 1) && automorphism < 2 * c.n, "invalid negacyclic automorphism index");
+    const size_t slot_words = host_slot_words(c, level, chunk, rotate);
+    const size_t need = 2 * aligned_bytes(slot_words) + workspace_bytes(c, NTT_B200_OP_KEYSWITCH, level, chunk);
+    if (!workspace || ws_size < need) throw WorkspaceError("workspace missing or too small");
+    DeviceGuard guard(c.device);
+    c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level));
+    c.down_plan(level);
+    std::lock_guard<std::mutex> lock(c.pipe_mu);
+    if (!c.copy_in) {
+      CUDA_CHECK(cudaStreamCreateWithFlags(&c.copy_in, cudaStreamNonBlocking));
+      CUDA_CHECK(cudaStreamCreateWithFlags(&c.copy_out, cudaStreamNonBlocking));
+      for (int i = 0; i < 2; ++i) {
+        CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_in[i], cudaEventDisableTiming));
+        CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_comp[i], cudaEventDisableTiming));
+        CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_out[i], cudaEventDisableTiming));
+      }
+      CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_start, cudaEventDisableTiming));
+    }
+    const cudaStream_t st = as_stream(stream);
+    char *base = reinterpret_cast<char *>(workspace);
+    u64 *slot[2] = {reinterpret_cast<u64 *>(base), reinterpret_cast<u64 *>(base + aligned_bytes(slot_words))};
+    char *ks_ws = base + 2 * aligned_bytes(slot_words);
+    const size_t ks_bytes = ws_size - 2 * aligned_bytes(slot_words);
+    const size_t poly = level * c.n;  // words per request and component
+    // The copy streams start after everything already on the caller's stream.
+    CUDA_CHECK(cudaEventRecord(c.ev_start, st));
+    CUDA_CHECK(cudaStreamWaitEvent(c.copy_in, c.ev_start, 0));
+    CUDA_CHECK(cudaStreamWaitEvent(c.copy_out, c.ev_start, 0));
+    for (size_t first = 0, k = 0; first < batch; first += chunk, ++k) {
+      const size_t r = std::min(chunk, batch - first);
+      const int sl = (int)(k & 1);
+      u64 *d_src = slot[sl], *d_b = d_src + chunk * poly, *d_a = d_b + chunk * poly;
+      u64 *d_c0 = rotate ? d_a + chunk * poly : nullptr;
+      // host -> device, once the compute two chunks back has read this slot
+      CUDA_CHECK(cudaStreamWaitEvent(c.copy_in, c.ev_comp[sl], 0));
+      CUDA_CHECK(cudaMemcpyAsync(d_src, h_src + first * poly, r * poly * sizeof(u64), cudaMemcpyHostToDevice,
+                                 c.copy_in));
+      if (rotate)
+        CUDA_CHECK(cudaMemcpyAsync(d_c0, h_c0 + first * poly, r * poly * sizeof(u64), cudaMemcpyHostToDevice,
+                                   c.copy_in));
+      CUDA_CHECK(cudaEventRecord(c.ev_in[sl], c.copy_in));
+      // compute on the caller's stream, once the inputs are in and the outputs
+      // of two chunks back have left for the host
+      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_in[sl], 0));
+      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[sl], 0));
+      Carver ws{ks_ws, ks_bytes};
+      do_keyswitch(c, level, r, d_b, d_a, d_src, key_b, key_a, d_c0, automorphism, ws, st);
+      CUDA_CHECK(cudaEventRecord(c.ev_comp[sl], st));
+      // device -> host
+      CUDA_CHECK(cudaStreamWaitEvent(c.copy_out, c.ev_comp[sl], 0));
+      CUDA_CHECK(cudaMemcpyAsync(h_out_b + first * poly, d_b, r * poly * sizeof(u64), cudaMemcpyDeviceToHost,
+                                 c.copy_out));
+      CUDA_CHECK(cudaMemcpyAsync(h_out_a + first * poly, d_a, r * poly * sizeof(u64), cudaMemcpyDeviceToHost,
+                                 c.copy_out));
+      CUDA_CHECK(cudaEventRecord(c.ev_out[sl], c.copy_out));
+    }
+    // The caller's stream continues once every output has reached the host.
+    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[0], 0));
+    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[1], 0));
   });
 }
 

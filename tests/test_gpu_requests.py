@@ -173,3 +173,29 @@ def test_request_contract_errors(lib, orc):
     with pytest.raises(nb.WorkspaceError):
         g.keyswitch_requests([a.request(), b.request()], ws[:16])
     g.close()
+
+
+@pytest.mark.parametrize("batch,chunk,rotate", [(7, 2, False), (7, 3, True), (2, 4, True), (5, 1, False)])
+def test_host_buffer_pipeline_matches_oracle(lib, orc, batch, chunk, rotate):
+    """ntt_b200_keyswitch_host: pinned host inputs and outputs, chunks through two
+    device slots with overlapped copies; two calls in a row on one stream."""
+    import torch
+    ctx = synthetic_context(orc, 8192, 6, 3, 2)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka, dkb, dka = _keys(orc, ctx, 61)
+    level = 5
+    ws = g.host_workspace(level, chunk, rotate)
+    for call in range(2):
+        xs = np.stack([orc.lcg(ctx.n, ctx.q[:level], 100 * call + r) for r in range(batch)])
+        c0 = np.stack([orc.lcg(ctx.n, ctx.q[:level], 500 + 100 * call + r) for r in range(batch)]) if rotate else None
+        h_x = torch.from_numpy(xs.view(np.int64)).pin_memory()
+        h_c0 = torch.from_numpy(c0.view(np.int64)).pin_memory() if rotate else None
+        h_b = torch.zeros(xs.shape, dtype=torch.int64).pin_memory()
+        h_a = torch.zeros(xs.shape, dtype=torch.int64).pin_memory()
+        g.keyswitch_host(level, batch, chunk, h_x, h_b, h_a, dkb, dka, ws, h_c0=h_c0, automorphism=25 if rotate else 0)
+        torch.cuda.synchronize()
+        for r in range(batch):
+            wb, wa = orc.keyswitch(ctx, level, xs[r], kb, ka, None if c0 is None else c0[r], 25 if rotate else 0)
+            np.testing.assert_array_equal(h_b[r].numpy().view(np.uint64), wb)
+            np.testing.assert_array_equal(h_a[r].numpy().view(np.uint64), wa)
+    g.close()
