@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "keyswitch/s N=2^16 L=24 dnum=3 served vs plain, p50/p99 ms; NTT HBM GB/s"
 UNIT = "keyswitch/s"
 N, LEVEL, K_P, DNUM, BATCH = 65536, 24, 8, 3, 16
-E2E_CHUNK = 2  # requests per chunk of the host-buffer pipeline
+E2E_CHUNK = 1  # requests per chunk of the host-buffer pipeline (best of 1, 2, 4, 8, 16 on a B200)
 SEED = 0x7251D9
 WORKLOAD = ("batched Hybrid key switch: 16 ciphertext components per GPU at N=2^16, L=24 (55-bit), "
             "K=8 (60-bit), dnum=3 (alpha=8), one shared switching key")
@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-vs-plain Poisson legs")
+    ap.add_argument("--rotate", action="store_true",
+                    help="profiling: every batched request also adds P*c0 and rotates by g = 5 (rotate kernel)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="timed batched steps only (no plain/e2e/CPU legs); for profiler launch lists")
     return ap.parse_args()
@@ -488,8 +490,11 @@ def run_ours(args, rank, world, local):
     ws = ctx.workspace(nb.OP_KEYSWITCH, LEVEL, B)
     stream = torch.cuda.current_stream(dev)
 
+    d_c0 = nb.to_device(uniform_residues(N, prm.q, SEED + 3 + 1000 * rank, polys=B), device) if args.rotate else None
+
     def step():
-        ctx.keyswitch_batch(LEVEL, B, out_b, out_a, d_x, d_kb, d_ka, ws, stream=stream)
+        ctx.keyswitch_batch(LEVEL, B, out_b, out_a, d_x, d_kb, d_ka, ws, c0=d_c0,
+                            automorphism=5 if args.rotate else 0, stream=stream)
 
     for _ in range(max(3, args.warmup)):
         step()
