@@ -90,6 +90,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",)),
         ("conv_limbs", (0, 1), ks_step, ("conv",)),
         ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",)),
+        ("mac_limbs", (0, 1), ks_step, ("mac",)),
     ]
     measurements, choices = {}, {}
     for name, candidates, step, judge in plan:

@@ -364,6 +364,7 @@ Tunable g_tuning[] = {
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
+    {"mac_limbs", {1}, 0, 1},          // 30-bit-limb MAC kernel where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
 };
 Tunable *find_tunable(const char *name) {
@@ -767,8 +768,17 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
   for (auto q : c.mod) max_q = std::max(max_q, q);
   const u128 prod = (u128)(max_q - 1) * (max_q - 1);
   const bool wide = prod > (~(u128)0) / (u128)beta;
+  const bool limbs = max_q < (u64(1) << 60) && tuned("mac_limbs") != 0;
   Timed t("mac", st);
-  if (n >= 2 * b200::kEwThreads && beta <= 4) {
+  if (n >= 2 * b200::kEwThreads && beta <= 4 && limbs) {
+    const dim3 grid2((unsigned)(n / (2 * b200::kEwThreads)), (unsigned)polys, (unsigned)T);
+    switch (beta) {
+      case 1: b200::mac2_limb_kernel<1><<<grid2, b200::kEwThreads, 0, st>>>(a); break;
+      case 2: b200::mac2_limb_kernel<2><<<grid2, b200::kEwThreads, 0, st>>>(a); break;
+      case 3: b200::mac2_limb_kernel<3><<<grid2, b200::kEwThreads, 0, st>>>(a); break;
+      default: b200::mac2_limb_kernel<4><<<grid2, b200::kEwThreads, 0, st>>>(a); break;
+    }
+  } else if (n >= 2 * b200::kEwThreads && beta <= 4) {
     const dim3 grid2((unsigned)(n / (2 * b200::kEwThreads)), (unsigned)polys, (unsigned)T);
     auto launch = [&](auto beta_tag) {
       constexpr int B = decltype(beta_tag)::value;

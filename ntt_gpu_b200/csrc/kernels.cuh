@@ -331,6 +331,68 @@ __global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
   *reinterpret_cast<ulonglong2 *>(a.out_a + o) = ra;
 }
 
+// Same MAC with 30-bit limbs, when every QP modulus is below 2^60 and
+// BETA <= 8: each product x * k = (x1*2^30 + x0)(k1*2^30 + k0) accumulates
+// into L += x0*k0, H += x1*k1 and M += (x0+x1)(k0+k1); the exact sum is
+// H*2^60 + (M - L - H)*2^30 + L (conv_limb_kernel's scheme: three multiply-adds
+// per product and no carry handling). Results equal mac2_kernel's bit for bit.
+template <int BETA>
+__global__ void __launch_bounds__(kEwThreads) mac2_limb_kernel(MacArgs a) {
+  constexpr u64 kMask30 = (u64(1) << 30) - 1;
+  const u64 n = u64(1) << a.logn;
+  const u64 i = (u64(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
+  const int t = blockIdx.z;
+  const u64 z = blockIdx.y;
+  if (i >= n) return;
+  const int g = t < a.level ? t : a.m + (t - a.level);
+  const Reducer red = a.tc[g].red;
+  const u64 row = (a.full_key_rows || a.req) ? u64(g) : u64(t);
+  const MacBases mb = mac_bases(a, z);
+  const int own = (mb.input && t < a.level) ? t / a.alpha : -1;
+  const u64 doff = mb.dz * a.poly_stride_digits + t * n + i;
+  // accumulators by (channel, coefficient): b.x, b.y, a.x, a.y
+  u64 lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0}, mid[4] = {0, 0, 0, 0};
+  auto mad = [&](int s, u64 x0, u64 x1, u64 xs, u64 k) {
+    const u64 k0 = k & kMask30, k1 = k >> 30;
+    lo[s] += (u64)(uint32_t)x0 * (uint32_t)k0;
+    hi[s] += (u64)(uint32_t)x1 * (uint32_t)k1;
+    mid[s] += (u64)(uint32_t)xs * (uint32_t)(k0 + k1);
+  };
+#pragma unroll
+  for (int j = 0; j < BETA; ++j) {
+    const ulonglong2 x = j == own ? *reinterpret_cast<const ulonglong2 *>(mb.input + t * n + i)
+                                  : *reinterpret_cast<const ulonglong2 *>(a.digit[j] + doff);
+    const u64 *kbp = a.req ? mb.kb + j * a.key_digit_stride : a.key_b[j];
+    const u64 *kap = a.req ? mb.ka + j * a.key_digit_stride : a.key_a[j];
+    const ulonglong2 kb = *reinterpret_cast<const ulonglong2 *>(kbp + row * n + i);
+    const ulonglong2 ka = *reinterpret_cast<const ulonglong2 *>(kap + row * n + i);
+    const u64 p0 = x.x & kMask30, p1 = x.x >> 30, q0 = x.y & kMask30, q1 = x.y >> 30;
+    mad(0, p0, p1, p0 + p1, kb.x);
+    mad(1, q0, q1, q0 + q1, kb.y);
+    mad(2, p0, p1, p0 + p1, ka.x);
+    mad(3, q0, q1, q0 + q1, ka.y);
+  }
+  u64 r[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    Acc128 v;
+    v.v = ((u128)hi[s] << 60) + ((u128)(mid[s] - lo[s] - hi[s]) << 30) + lo[s];
+    r[s] = reduce(v, red);
+  }
+  const u64 o = z * a.poly_stride_out + t * n + i;
+  ulonglong2 rb = make_ulonglong2(r[0], r[1]), ra = make_ulonglong2(r[2], r[3]);
+  if (a.accumulate) {
+    const ulonglong2 ob = *reinterpret_cast<const ulonglong2 *>(a.out_b + o);
+    const ulonglong2 oa = *reinterpret_cast<const ulonglong2 *>(a.out_a + o);
+    rb.x = add_mod(rb.x, ob.x, red.m);
+    rb.y = add_mod(rb.y, ob.y, red.m);
+    ra.x = add_mod(ra.x, oa.x, red.m);
+    ra.y = add_mod(ra.y, oa.y, red.m);
+  }
+  *reinterpret_cast<ulonglong2 *>(a.out_b + o) = rb;
+  *reinterpret_cast<ulonglong2 *>(a.out_a + o) = ra;
+}
+
 // ---- rotation: automorphism gather plus P*c0 on Q towers ------------------------
 // resident_adapter.inc:44-59 semantics with automorphism_source_index and
 // rotated_b_value (resident_conversion.hpp:15-29).
