@@ -364,7 +364,7 @@ Tunable g_tuning[] = {
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
-    {"mac_limbs", {1}, 0, 1},          // 30-bit-limb MAC kernel where it applies
+    {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
 };
 Tunable *find_tunable(const char *name) {
