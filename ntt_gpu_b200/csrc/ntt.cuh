@@ -269,6 +269,31 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
 // (one pad word per 16) so both mappings are bank-conflict free.
 __device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
 
+// Warp-local copies between global memory and a warp's two padded tile rows
+// (rows 2w and 2w+1 of the tile belong to warp w in both row passes): 16-byte
+// coalesced chunks and no CTA-wide barrier, so the warps of a CTA run their
+// load, butterfly and store phases independently and overlap one another.
+__device__ __forceinline__ void load_rows_warp(u64 *tile, const u64 *g) {
+  const int lane = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 2;
+#pragma unroll
+  for (int j = lane; j < 256; j += 32) {
+    const int rr = r0 + (j >> 7), c = (j & 127) * 2;
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(g + rr * 256 + c);
+    const int sidx = rr * kRowPad + pad_col(c);
+    tile[sidx] = v.x;
+    tile[sidx + 1] = v.y;
+  }
+}
+__device__ __forceinline__ void store_rows_warp(u64 *g, const u64 *tile) {
+  const int lane = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 2;
+#pragma unroll
+  for (int j = lane; j < 256; j += 32) {
+    const int rr = r0 + (j >> 7), c = (j & 127) * 2;
+    const int sidx = rr * kRowPad + pad_col(c);
+    *reinterpret_cast<ulonglong2 *>(g + rr * 256 + c) = make_ulonglong2(tile[sidx], tile[sidx + 1]);
+  }
+}
+
 // Twiddle staging for the row passes' register-bit stages (s' = 4..7, where
 // lane u of row r needs T[2^s + (row << s') + ((16u + e) >> (8 - s'))]): with STW
 // set, the CTA first copies the stage's 16 * 2^s' twiddles, contiguous in the
@@ -294,8 +319,13 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
-  load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
-  __syncthreads();
+  if constexpr (STW) {
+    load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
+    __syncthreads();
+  } else {
+    load_rows_warp(tile, v.src + row0 * 256);
+    __syncwarp();
+  }
   const int r = threadIdx.x / 16, u = threadIdx.x % 16;
   const int row = row0 + r;
   u64 *my = tile + r * kRowPad;
@@ -353,9 +383,16 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
     x[e] = reduce_final<MODE>(x[e], q, q2);
     my[pad_col(u * 16 + e)] = x[e];
   }
-  __syncthreads();
+  if constexpr (STW) {
+    __syncthreads();
+  } else {
+    __syncwarp();
+  }
   if (b.epi_left == nullptr) {
-    store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+    if constexpr (STW)
+      store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+    else
+      store_rows_warp(v.dst + row0 * 256, tile);
     return;
   }
   const u64 *left = b.epi_left + blockIdx.z * b.epi_left_stride + u64(b.off[blockIdx.y]) * (u64(1) << T.logn) +
@@ -364,7 +401,12 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   u64 *out = v.dst + row0 * 256;
   const u64 *add = poly_add(b, blockIdx.z);
   if (add) add += u64(b.off[blockIdx.y]) * (u64(1) << T.logn) + row0 * 256;
-  for (int j = threadIdx.x; j < 16 * 128; j += kNttThreads) {
+  // Epilogue over the rows this thread's group owns: every row with STW (the
+  // CTA synchronised above), the warp's own two rows otherwise.
+  const int j0 = STW ? int(threadIdx.x) : int(threadIdx.x & 31) + (int(threadIdx.x >> 5) * 2) * 128;
+  const int j1 = STW ? 16 * 128 : j0 - int(threadIdx.x & 31) + 2 * 128;
+  const int jstep = STW ? kNttThreads : 32;
+  for (int j = j0; j < j1; j += jstep) {
     const int rr = j >> 7, c = (j & 127) * 2;
     const int sidx = rr * kRowPad + pad_col(c);
     const ulonglong2 l = *reinterpret_cast<const ulonglong2 *>(left + rr * 256 + c);
@@ -387,8 +429,13 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
   const TowerView v = tower_view(b, T, true);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
-  load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
-  __syncthreads();
+  if constexpr (STW) {
+    load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
+    __syncthreads();
+  } else {
+    load_rows_warp(tile, v.src + row0 * 256);
+    __syncwarp();
+  }
   const int r = threadIdx.x / 16, u = threadIdx.x % 16;
   const int row = row0 + r;
   u64 *my = tile + r * kRowPad;
@@ -443,8 +490,13 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
   }
 #pragma unroll
   for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
-  __syncthreads();
-  store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+  if constexpr (STW) {
+    __syncthreads();
+    store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+  } else {
+    __syncwarp();
+    store_rows_warp(v.dst + row0 * 256, tile);
+  }
 }
 
 // ---- small transforms (N <= 2048): one CTA per tower, strict arithmetic -------
