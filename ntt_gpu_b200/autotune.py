@@ -14,7 +14,7 @@ workloads:
                K = 8, dnum = 3.
 
 Each candidate is timed with the library's per-kernel CUDA-event timing
-(ntt_b200_timing_*), so a pass's choice is judged by that pass's own device time.
+(ntt_b200_timing_*), so each choice is measured by the device time of the pass it affects.
 The choices and every measurement are written to ntt_gpu_b200/tuning.json,
 which ntt_gpu_b200.load() applies.
 
@@ -79,7 +79,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         kctx.keyswitch_batch(24, batch, ob, oa, xs, kb, ka, ws)
 
     passes = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col")
-    # tunable -> (candidates, workload, kernel classes that judge it)
+    # tunable -> (candidates, workload, kernel classes whose device time decides it)
     plan = [
         ("ntt_persistent", (0, 1), ntt_step, passes),
         ("ntt_minb_fwd_col", (3, 4), ntt_step, ("ntt_fwd_col",)),
@@ -93,15 +93,15 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("mac_limbs", (0, 1), ks_step, ("mac",)),
     ]
     measurements, choices = {}, {}
-    for name, candidates, step, judge in plan:
+    for name, candidates, step, kernels in plan:
         times = {}
         for value in candidates:
             nb.tuning_set(name, value)
-            times[value] = sum(_device_ms(nb, torch, step, iters, judge).values())
+            times[value] = sum(_device_ms(nb, torch, step, iters, kernels).values())
         best = min(times, key=times.get)
         nb.tuning_set(name, best)
         choices[name] = best
-        measurements[name] = {"judged_by": list(judge), "device_ms_per_call": {str(k): v for k, v in times.items()}}
+        measurements[name] = {"measured_by": list(kernels), "device_ms_per_call": {str(k): v for k, v in times.items()}}
 
     def total(step):
         torch.cuda.synchronize()
