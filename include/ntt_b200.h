@@ -67,6 +67,9 @@ int ntt_b200_context_table_bytes(ntt_b200_context ctx, size_t *out);
 /* Build every conversion/correction plan a key switch at `level` needs, so that
  * later calls at that level perform no host work or table upload. */
 int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level);
+/* Nonzero `count` when a kernel of this context gave up a bounded wait on the
+ * GPU (its results are then invalid); a synchronous read, `clear` resets it. */
+int ntt_b200_device_errors(ntt_b200_context ctx, int *count, int clear);
 /* Words of one channel of a full-context switching key: digits x (M + K) x N
  * (the packing of Session::upload_hybrid_key's source, src/resident.cpp:492-529). */
 int ntt_b200_context_key_words(ntt_b200_context ctx, size_t *words);

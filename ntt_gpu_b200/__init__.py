@@ -77,6 +77,7 @@ _SIGNATURES = {
     "ntt_b200_server_destroy": ([_P], _I),
     "ntt_b200_server_attach_keycache": ([_P, _P], _I),
     "ntt_b200_context_key_words": ([_P, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_device_errors": ([_P, ctypes.POINTER(_I), _I], _I),
     "ntt_b200_keycache_last_error": ([], ctypes.c_char_p),
     "ntt_b200_keycache_create": ([ctypes.POINTER(_P), _I, _SZ], _I),
     "ntt_b200_keycache_destroy": ([_P], _I),
@@ -271,6 +272,12 @@ class Context:
 
     def qp_ids(self, level):
         return list(range(level)) + [self.m + j for j in range(self.k)]
+
+    def device_errors(self, clear=False) -> int:
+        """Count of expired bounded waits on the GPU (0 when every kernel completed normally)."""
+        out = _I()
+        _check(self._lib.ntt_b200_device_errors(self._h, ctypes.byref(out), int(clear)))
+        return out.value
 
     def table_bytes(self) -> int:
         out = _SZ()

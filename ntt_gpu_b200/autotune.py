@@ -4,7 +4,8 @@ Every tunable (ntt_b200_tuning_name) is a launch choice that never changes a
 result: the NTT pass variant (one CTA per tile, or persistent and double
 buffered), the register budget each NTT pass is compiled for (3 or 4 resident
 CTAs per SM), whether the row passes stage their twiddles in shared memory, the
-conversion kernel (30-bit limbs or 128-bit accumulators) and
+conversion kernel (tensor cores, 30-bit limbs or 128-bit accumulators), the MAC
+kernel and
 the conversion grid target. The tuner runs coordinate descent over them on two
 workloads:
 
@@ -91,6 +92,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("conv_limbs", (0, 1), ks_step, ("conv",)),
         ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",)),
         ("mac_limbs", (0, 1), ks_step, ("mac",)),
+        ("conv_tc", (0, 1), ks_step, ("conv",)),
     ]
     measurements, choices = {}, {}
     for name, candidates, step, kernels in plan:

@@ -139,6 +139,10 @@ struct HostConvPlan {
   int s = 0, t = 0;
   bool wide = false;
   bool limb = false;  // all moduli < 2^60 and s <= 8: the 30-bit-limb kernel applies
+  // Tensor-core form (s <= 16): byte limbs of [Bhat_jt * 2^(8a)]_{m_t} in the
+  // canonical K-major layout, groups of 8 targets x 8 output bytes.
+  uint8_t *tc_b = nullptr;
+  int tc_kpad = 0, tc_groups = 0;
 };
 }  // namespace
 
@@ -150,6 +154,7 @@ struct ntt_b200_context_s {
   int mode = 2;  // NTT butterfly mode: 2 all moduli < 2^61, 1 all < 2^62, 0 otherwise
   std::vector<u64> mod, psi;  // [M + K] by global id
   b200::TowerConsts *d_tc = nullptr;
+  int *d_err = nullptr;  // set by kernels whose bounded waits expired (read by ntt_b200_device_errors)
   ulonglong2 *d_fwd = nullptr, *d_inv = nullptr;
   b200::DeviceTables tables{};
   size_t table_bytes = 0;
@@ -170,7 +175,11 @@ struct ntt_b200_context_s {
     // Destruction requires quiescence: the caller has synchronised every stream
     // that used this context (the reference frees tables only after proven
     // quiescence, src/cuda/resident_adapter.inc:107-115).
-    for (auto &kv : conv) cudaFree(kv.second.device);
+    for (auto &kv : conv) {
+      cudaFree(kv.second.device);
+      if (kv.second.tc_b) cudaFree(kv.second.tc_b);
+    }
+    if (d_err) cudaFree(d_err);
     for (auto &kv : down) cudaFree(kv.second);
     if (copy_in) cudaStreamDestroy(copy_in);
     if (copy_out) cudaStreamDestroy(copy_out);
@@ -230,6 +239,28 @@ struct ntt_b200_context_s {
     DeviceGuard guard(device);
     CUDA_CHECK(cudaMalloc(&hp.device, sizeof(b200::ConvPlan)));
     CUDA_CHECK(cudaMemcpy(hp.device, plan.get(), sizeof(b200::ConvPlan), cudaMemcpyHostToDevice));
+    if (s <= 16 && n >= (u64)b200::kTcThreads) {
+      // B rows n' = 8 * (target within its group) + output byte b, columns
+      // k' = 8 * source + input byte a: byte b of [Bhat_jt * 2^(8a)]_{m_t}.
+      hp.tc_kpad = (8 * s + 31) / 32 * 32;
+      hp.tc_groups = (t + b200::kTcGroupTargets - 1) / b200::kTcGroupTargets;
+      const int rows = b200::kTcGroupRows, kpad = hp.tc_kpad;
+      std::vector<uint8_t> bm((size_t)hp.tc_groups * rows * kpad, 0);
+      for (int i = 0; i < t; ++i) {
+        const u64 m_i = mod[tgt[i]];
+        const int g = i / b200::kTcGroupTargets, tl = i % b200::kTcGroupTargets;
+        for (int j = 0; j < s; ++j) {
+          u64 c = plan->hat[j * t + i] % m_i;  // [Bhat_jt]_{m_t} * 2^(8a), a = 0..7
+          for (int a = 0; a < 8; ++a) {
+            for (int b = 0; b < 8; ++b)
+              bm[(size_t)g * rows * kpad + b200::tc_canon(tl * 8 + b, j * 8 + a, rows)] = (uint8_t)(c >> (8 * b));
+            c = h_mul(c, 256 % m_i, m_i);
+          }
+        }
+      }
+      CUDA_CHECK(cudaMalloc(&hp.tc_b, bm.size()));
+      CUDA_CHECK(cudaMemcpy(hp.tc_b, bm.data(), bm.size(), cudaMemcpyHostToDevice));
+    }
     return conv.emplace(key, hp).first->second;
   }
 
@@ -365,6 +396,7 @@ Tunable g_tuning[] = {
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
     {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
+    {"conv_tc", {0}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
 };
 Tunable *find_tunable(const char *name) {
@@ -599,12 +631,48 @@ void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, bo
   else
     b200::conv_kernel<MAXS, false, false><<<grid, b200::kEwThreads, 0, st>>>(a);
 }
+void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, const std::vector<uint16_t> &slots,
+                 size_t polys, u64 src_stride, u64 dst_stride, cudaStream_t st, bool lazy_out) {
+  b200::ConvTcArgs a{};
+  a.plan = p.device;
+  a.bmat = p.tc_b;
+  a.src = src;
+  a.dst = dst;
+  a.src_poly_stride = src_stride;
+  a.dst_poly_stride = dst_stride;
+  for (size_t i = 0; i < slots.size(); ++i) a.slot[i] = slots[i];
+  a.logn = c.logn;
+  a.kpad = p.tc_kpad;
+  a.groups = p.tc_groups;
+  a.err = c.d_err;
+  const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad;
+  static int attr_set[64][2] = {};
+  auto launch = [&](auto kernel, int which) {
+    if (!attr_set[c.device][which]) {
+      CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+      attr_set[c.device][which] = 1;
+    }
+    const dim3 grid((unsigned)(c.n / b200::kTcThreads), 1, (unsigned)polys);
+    Timed t("conv", st);
+    kernel<<<grid, b200::kTcThreads, smem, st>>>(a);
+    t.done();
+  };
+  if (lazy_out)
+    launch(b200::conv_tc_kernel<true>, 1);
+  else
+    launch(b200::conv_tc_kernel<false>, 0);
+}
+
 // lazy_out: outputs in [0, 4m), only for a lazy forward NTT that consumes them.
 void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
               const std::vector<uint16_t> &slots, size_t polys, u64 src_stride, u64 dst_stride,
               cudaStream_t st, bool lazy_out = false) {
   lazy_out = lazy_out && c.mode >= 1 && c.logn >= 12;
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
+  if (p.tc_b && tuned("conv_tc") != 0) {
+    run_conv_tc(c, p, dst, src, slots, polys, src_stride, dst_stride, st, lazy_out);
+    return;
+  }
   b200::ConvArgs a{};
   a.plan = p.device;
   a.src = src;
@@ -1150,6 +1218,8 @@ int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const
     }
     DeviceGuard guard(device);
     CUDA_CHECK(cudaMalloc(&c->d_tc, T * sizeof(b200::TowerConsts)));
+    CUDA_CHECK(cudaMalloc(&c->d_err, sizeof(int)));
+    CUDA_CHECK(cudaMemset(c->d_err, 0, sizeof(int)));
     CUDA_CHECK(cudaMalloc(&c->d_fwd, T * n * sizeof(ulonglong2)));
     CUDA_CHECK(cudaMalloc(&c->d_inv, T * n * sizeof(ulonglong2)));
     CUDA_CHECK(cudaMemcpy(c->d_tc, tc.data(), T * sizeof(b200::TowerConsts), cudaMemcpyHostToDevice));
@@ -1174,6 +1244,16 @@ int ntt_b200_context_table_bytes(ntt_b200_context ctx, size_t *out) {
     require_ctx(ctx);
     require(out != nullptr, "null output");
     *out = ctx->table_bytes;
+  });
+}
+
+int ntt_b200_device_errors(ntt_b200_context ctx, int *count, int clear) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(count != nullptr, "null output");
+    DeviceGuard guard(ctx->device);
+    CUDA_CHECK(cudaMemcpy(count, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (clear) CUDA_CHECK(cudaMemset(ctx->d_err, 0, sizeof(int)));
   });
 }
 

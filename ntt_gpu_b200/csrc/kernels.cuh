@@ -162,6 +162,155 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
   }
 }
 
+// ---- approximate-CRT switch on the tensor cores (tcgen05, unsigned int8) -----------
+// For a target m_t the output only has to be congruent to sum_j y_j * Bhat_jt
+// modulo m_t. With y_j = sum_a y_ja 2^(8a) (byte limbs) and the precomputed
+// c_jat = [Bhat_jt * 2^(8a)]_{m_t} = sum_b c_jatb 2^(8b):
+//   sum_j y_j Bhat_jt == sum_b 2^(8b) S_tb  (mod m_t),  S_tb = sum_{j,a} y_ja c_jatb,
+// and every S_tb is a plain dot product of bytes (at most 128 terms of 255^2,
+// below 2^23): one [128 coefficients x 8s] x [8s x 8 per target] unsigned int8
+// matrix product with int32 accumulators in tensor memory. Each thread then
+// combines its coefficient's eight S_tb per target into an integer below 2^80
+// and reduces it modulo m_t, which gives the same residue as conv_kernel.
+//
+// CTA = 128 threads = 128 coefficients = the 128 TMEM lanes. A: one row of
+// 8s bytes per coefficient. B: groups of 8 targets (64 rows of 8s bytes),
+// built on the host per plan. Both use the canonical K-major layout without
+// swizzle: core matrices of 8 rows x 16 bytes stored as [k chunk][row group]
+// [8 rows][16 B], so SBO = 128 B and LBO = (rows / 8) * 128 B. Targets run in
+// groups of 8 through 64 TMEM columns; the MMA completion wait is bounded and
+// a timeout is reported through `err` (results of that CTA are then invalid).
+constexpr int kTcThreads = 128;
+constexpr int kTcGroupTargets = 8;
+constexpr int kTcGroupRows = 64;  // 8 targets x 8 output bytes
+struct ConvTcArgs {
+  const ConvPlan *plan;
+  const uint8_t *bmat;  // [groups][64 rows x kpad] bytes, canonical layout
+  const u64 *src;
+  u64 *dst;
+  u64 src_poly_stride, dst_poly_stride;
+  uint16_t slot[kMaxConvTargets];
+  int logn, kpad, groups;
+  int *err;
+};
+
+__host__ __device__ __forceinline__ int tc_canon(int r, int k, int rows) {
+  return ((k >> 4) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 15);
+}
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// Shared-memory matrix descriptor: SWIZZLE_NONE, Blackwell version 1.
+__device__ __forceinline__ u64 tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return u64((addr >> 4) & 0x3FFF) | (u64((lbo >> 4) & 0x3FFF) << 16) | (u64((sbo >> 4) & 0x3FFF) << 32) |
+         (u64(1) << 46);
+}
+
+template <bool LAZY_OUT>
+__global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) u64 mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ Reducer red[kMaxConvTargets];
+  __shared__ u64 sq[kMaxConvSources];
+  __shared__ Shoup sinv[kMaxConvSources];
+  const ConvPlan &p = *a.plan;
+  const int s = p.s, t_count = p.t, kpad = a.kpad;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  uint8_t *sa = tc_smem;                      // 128 x kpad
+  uint8_t *sb = tc_smem + kTcThreads * kpad;  // groups x 64 x kpad
+  // B groups (16-byte copies; the host built them in canonical order).
+  const int bbytes = a.groups * kTcGroupRows * kpad;
+  for (int i = tid * 16; i < bbytes; i += kTcThreads * 16)
+    *reinterpret_cast<uint4 *>(sb + i) = *reinterpret_cast<const uint4 *>(a.bmat + i);
+  for (int t = tid; t < t_count; t += kTcThreads) red[t] = p.tgt[t];
+  for (int j = tid; j < s; j += kTcThreads) {
+    sq[j] = p.src_q[j];
+    sinv[j] = p.src_inv[j];
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
+                 "r"(kTcGroupRows));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncthreads();
+  // A row of this thread's coefficient: the byte limbs of y_j, zero-padded.
+  const u64 n = u64(1) << a.logn;
+  const u64 k = u64(blockIdx.x) * kTcThreads + tid;
+  const u64 *src = a.src + blockIdx.z * a.src_poly_stride;
+  for (int j = 0; j < kpad / 8; ++j) {
+    const u64 y = j < s ? shoup_canon(src[u64(j) * n + k], sinv[j].w, sinv[j].wq, sq[j]) : 0;
+    *reinterpret_cast<u64 *>(sa + tc_canon(tid, j * 8, kTcThreads)) = y;  // little-endian bytes = limbs
+  }
+  asm volatile("fence.proxy.async.shared::cta;");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  // idesc: S32 accumulate, unsigned 8-bit A and B, K-major, N = 64, M = 128.
+  const uint32_t idesc = (2u << 4) | (uint32_t(kTcGroupRows >> 3) << 17) | (uint32_t(kTcThreads >> 4) << 24);
+  u64 *dst = a.dst + blockIdx.z * a.dst_poly_stride;
+  bool ok = true;
+  for (int g = 0; g < a.groups; ++g) {
+    if (tid == 0) {
+      for (int i = 0; i < kpad / 32; ++i) {
+        const u64 da = tc_desc(smem_addr(sa) + i * 2 * (kTcThreads / 8) * 128, (kTcThreads / 8) * 128, 128);
+        const u64 db = tc_desc(smem_addr(sb + g * kTcGroupRows * kpad) + i * 2 * (kTcGroupRows / 8) * 128,
+                               (kTcGroupRows / 8) * 128, 128);
+        const uint32_t acc = i > 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_addr(&mbar)));
+    }
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 20) && !done; ++it)
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}\n"
+          : "=r"(done)
+          : "r"(smem_addr(&mbar)), "r"(uint32_t(g & 1)));
+    // One decision for the whole CTA: every thread leaves together on a timeout.
+    const bool all_done = __syncthreads_and(done != 0);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!all_done) {
+      ok = false;
+      break;
+    }
+    const int tl_end = min(kTcGroupTargets, t_count - g * kTcGroupTargets);
+    for (int tl = 0; tl < tl_end; ++tl) {
+      uint32_t v[8];
+      const uint32_t addr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(tl * 8);
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                     "=r"(v[7])
+                   : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;");
+      const u64 lo4 = u64(v[0]) + (u64(v[1]) << 8) + (u64(v[2]) << 16) + (u64(v[3]) << 24);
+      const u64 hi4 = u64(v[4]) + (u64(v[5]) << 8) + (u64(v[6]) << 16) + (u64(v[7]) << 24);
+      Acc128 acc;
+      acc.v = (u128)lo4 + ((u128)hi4 << 32);
+      const int t = g * kTcGroupTargets + tl;
+      dst[u64(a.slot[t]) * n + k] = reduce_out<LAZY_OUT>(acc, red[t]);
+    }
+    // Every lane's loads are done before the next group's MMA reuses the columns.
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+  }
+  if (!ok) atomicExch(a.err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcGroupRows));
+}
+
 // ---- ModDown tail: (l - r) * [P^-1]_q  (resident_conversion.hpp:45-49) ---------
 struct CorrectArgs {
   u64 *dst, *dst_odd;  // dst_odd set: polynomial z writes (z odd ? dst_odd : dst) + (z / 2) * stride
