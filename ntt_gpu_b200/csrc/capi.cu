@@ -228,6 +228,7 @@ struct ntt_b200_context_s {
     for (int i = 0; i < t; ++i) {
       plan->tgt_id[i] = tgt[i];
       plan->tgt[i] = h_reducer(mod[tgt[i]]);
+      plan->tc_wq32[i] = (u64)((((u128)1) << 96) / mod[tgt[i]]);  // fits: m_i > 2^32
       max_tgt = std::max(max_tgt, mod[tgt[i]]);
     }
     HostConvPlan hp;
@@ -239,7 +240,10 @@ struct ntt_b200_context_s {
     DeviceGuard guard(device);
     CUDA_CHECK(cudaMalloc(&hp.device, sizeof(b200::ConvPlan)));
     CUDA_CHECK(cudaMemcpy(hp.device, plan.get(), sizeof(b200::ConvPlan), cudaMemcpyHostToDevice));
-    if (s <= 16 && n >= (u64)b200::kTcThreads) {
+    // The tensor-core form's reduction needs 2^48 <= m_t < 2^61 (see conv_tc_kernel).
+    u64 min_tgt = ~u64(0);
+    for (int i = 0; i < t; ++i) min_tgt = std::min(min_tgt, mod[tgt[i]]);
+    if (s <= 16 && n >= (u64)b200::kTcThreads && min_tgt >= (u64(1) << 48) && max_tgt < (u64(1) << 61)) {
       // B rows n' = 8 * (target within its group) + output byte b, columns
       // k' = 8 * source + input byte a: byte b of [Bhat_jt * 2^(8a)]_{m_t}.
       hp.tc_kpad = (8 * s + 31) / 32 * 32;
@@ -396,7 +400,7 @@ Tunable g_tuning[] = {
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
     {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
-    {"conv_tc", {0}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
+    {"conv_tc", {1}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
 };
 Tunable *find_tunable(const char *name) {

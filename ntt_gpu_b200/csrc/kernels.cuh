@@ -169,9 +169,12 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 //   sum_j y_j Bhat_jt == sum_b 2^(8b) S_tb  (mod m_t),  S_tb = sum_{j,a} y_ja c_jatb,
 // and every S_tb is a plain dot product of bytes (at most 128 terms of 255^2,
 // below 2^23): one [128 coefficients x 8s] x [8s x 8 per target] unsigned int8
-// matrix product with int32 accumulators in tensor memory. Each thread then
-// combines its coefficient's eight S_tb per target into an integer below 2^80
-// and reduces it modulo m_t, which gives the same residue as conv_kernel.
+// matrix product with int32 accumulators in tensor memory. Each thread folds
+// its coefficient's eight S_tb per target into H * 2^32 + L (H, L < 2^47) and
+// reduces with one approximate-quotient Shoup product, (H * 2^32 mod m_t) in
+// [0, 4m) plus L, below 5m when 2^48 <= m_t < 2^61; the result is then brought
+// to [0, 4m) (lazy output) or to [0, m). It is congruent to conv_kernel's
+// output modulo m_t, hence identical once canonical.
 //
 // CTA = 128 threads = 128 coefficients = the 128 TMEM lanes. A: one row of
 // 8s bytes per coefficient. B: groups of 8 targets (64 rows of 8s bytes),
@@ -211,7 +214,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   extern __shared__ __align__(1024) uint8_t tc_smem[];
   __shared__ __align__(8) u64 mbar;
   __shared__ uint32_t tmem_base;
-  __shared__ Reducer red[kMaxConvTargets];
+  __shared__ u64 tm[kMaxConvTargets], twq[kMaxConvTargets];
   __shared__ u64 sq[kMaxConvSources];
   __shared__ Shoup sinv[kMaxConvSources];
   const ConvPlan &p = *a.plan;
@@ -223,7 +226,10 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   const int bbytes = a.groups * kTcGroupRows * kpad;
   for (int i = tid * 16; i < bbytes; i += kTcThreads * 16)
     *reinterpret_cast<uint4 *>(sb + i) = *reinterpret_cast<const uint4 *>(a.bmat + i);
-  for (int t = tid; t < t_count; t += kTcThreads) red[t] = p.tgt[t];
+  for (int t = tid; t < t_count; t += kTcThreads) {
+    tm[t] = p.tgt[t].m;
+    twq[t] = p.tc_wq32[t];
+  }
   for (int j = tid; j < s; j += kTcThreads) {
     sq[j] = p.src_q[j];
     sinv[j] = p.src_inv[j];
@@ -285,20 +291,35 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
       break;
     }
     const int tl_end = min(kTcGroupTargets, t_count - g * kTcGroupTargets);
-    for (int tl = 0; tl < tl_end; ++tl) {
-      uint32_t v[8];
-      const uint32_t addr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(tl * 8);
-      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                     "=r"(v[7])
-                   : "r"(addr));
+    // Four targets' 8 columns per load, one wait per load.
+    for (int tq = 0; tq < kTcGroupTargets; tq += 4) {
+      if (tq >= tl_end) break;
+      uint32_t v[32];
+      const uint32_t addr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(tq * 8);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(addr));
       asm volatile("tcgen05.wait::ld.sync.aligned;");
-      const u64 lo4 = u64(v[0]) + (u64(v[1]) << 8) + (u64(v[2]) << 16) + (u64(v[3]) << 24);
-      const u64 hi4 = u64(v[4]) + (u64(v[5]) << 8) + (u64(v[6]) << 16) + (u64(v[7]) << 24);
-      Acc128 acc;
-      acc.v = (u128)lo4 + ((u128)hi4 << 32);
-      const int t = g * kTcGroupTargets + tl;
-      dst[u64(a.slot[t]) * n + k] = reduce_out<LAZY_OUT>(acc, red[t]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int tl = tq + u;
+        if (tl >= tl_end) break;
+        const uint32_t *w = v + 8 * u;
+        const u64 lo4 = u64(w[0]) + (u64(w[1]) << 8) + (u64(w[2]) << 16) + (u64(w[3]) << 24);
+        const u64 hi4 = u64(w[4]) + (u64(w[5]) << 8) + (u64(w[6]) << 16) + (u64(w[7]) << 24);
+        const int t = g * kTcGroupTargets + tl;
+        const u64 m = tm[t];
+        // hi4 * 2^32 mod m in [0, 4m) (w = 2^32 < m), plus lo4 < 2^47 <= m: below 5m.
+        u64 r = shoup_approx(hi4, u64(1) << 32, twq[t], 0 - m) + lo4;
+        r = csub_sign(r, 4 * m);  // [0, 4m)
+        if constexpr (!LAZY_OUT) r = csub_sign(csub_sign(r, 2 * m), m);
+        dst[u64(a.slot[t]) * n + k] = r;
+      }
     }
     // Every lane's loads are done before the next group's MMA reuses the columns.
     asm volatile("tcgen05.fence::before_thread_sync;");

@@ -42,6 +42,7 @@ struct ConvPlan {
   uint16_t tgt_id[kMaxConvTargets];
   Reducer tgt[kMaxConvTargets];
   u64 hat[kMaxConvSources * kMaxConvTargets];  // [j][i] = Bhat_j mod m_i
+  u64 tc_wq32[kMaxConvTargets];                 // floor(2^96 / m_i): Shoup quotient of 2^32 mod m_i (m_i > 2^32)
 };
 
 // ModDown tail constants for one level: per Q tower [P^-1]_q and [P]_q.
