@@ -656,7 +656,8 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
       CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
       attr_set[c.device][which] = 1;
     }
-    const dim3 grid((unsigned)(c.n / b200::kTcThreads), 1, (unsigned)polys);
+    const size_t tiles = c.n / b200::kTcThreads;
+    const dim3 grid((unsigned)((tiles + b200::kTcTilesPerCta - 1) / b200::kTcTilesPerCta), 1, (unsigned)polys);
     Timed t("conv", st);
     kernel<<<grid, b200::kTcThreads, smem, st>>>(a);
     t.done();

@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 constexpr int kTcThreads = 128;
 constexpr int kTcGroupTargets = 8;
 constexpr int kTcGroupRows = 64;  // 8 targets x 8 output bytes
+constexpr int kTcTilesPerCta = 4;  // coefficient tiles per CTA (B, TMEM and barriers set up once)
 struct ConvTcArgs {
   const ConvPlan *plan;
   const uint8_t *bmat;  // [groups][64 rows x kpad] bytes, canonical layout
@@ -212,7 +213,7 @@ __device__ __forceinline__ u64 tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo
 template <bool LAZY_OUT>
 __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   extern __shared__ __align__(1024) uint8_t tc_smem[];
-  __shared__ __align__(8) u64 mbar;
+  __shared__ __align__(8) u64 mbar, bbar;
   __shared__ uint32_t tmem_base;
   __shared__ u64 tm[kMaxConvTargets], twq[kMaxConvTargets];
   __shared__ u64 sq[kMaxConvSources];
@@ -222,10 +223,20 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   const int tid = threadIdx.x, warp = tid >> 5;
   uint8_t *sa = tc_smem;                      // 128 x kpad
   uint8_t *sb = tc_smem + kTcThreads * kpad;  // groups x 64 x kpad
-  // B groups (16-byte copies; the host built them in canonical order).
-  const int bbytes = a.groups * kTcGroupRows * kpad;
-  for (int i = tid * 16; i < bbytes; i += kTcThreads * 16)
-    *reinterpret_cast<uint4 *>(sb + i) = *reinterpret_cast<const uint4 *>(a.bmat + i);
+  const uint32_t bbytes = uint32_t(a.groups * kTcGroupRows * kpad);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    // B (built on the host in canonical order) arrives by one bulk copy while
+    // the first tile's A rows are computed; 16-byte aligned, size a multiple of 16.
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bbar)), "r"(bbytes));
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(sb)),
+        "l"(a.bmat), "r"(bbytes), "r"(smem_addr(&bbar))
+        : "memory");
+  }
   for (int t = tid; t < t_count; t += kTcThreads) {
     tm[t] = p.tgt[t].m;
     twq[t] = p.tc_wq32[t];
@@ -239,94 +250,111 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
                  "r"(kTcGroupRows));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;");
-  }
   __syncthreads();
-  // A row of this thread's coefficient: the byte limbs of y_j, zero-padded.
-  const u64 n = u64(1) << a.logn;
-  const u64 k = u64(blockIdx.x) * kTcThreads + tid;
-  const u64 *src = a.src + blockIdx.z * a.src_poly_stride;
-  for (int j = 0; j < kpad / 8; ++j) {
-    const u64 y = j < s ? shoup_canon(src[u64(j) * n + k], sinv[j].w, sinv[j].wq, sq[j]) : 0;
-    *reinterpret_cast<u64 *>(sa + tc_canon(tid, j * 8, kTcThreads)) = y;  // little-endian bytes = limbs
-  }
-  asm volatile("fence.proxy.async.shared::cta;");
-  asm volatile("tcgen05.fence::before_thread_sync;");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
+  const u64 n = u64(1) << a.logn;
+  const u64 *src = a.src + blockIdx.z * a.src_poly_stride;
+  u64 *dst = a.dst + blockIdx.z * a.dst_poly_stride;
   // idesc: S32 accumulate, unsigned 8-bit A and B, K-major, N = 64, M = 128.
   const uint32_t idesc = (2u << 4) | (uint32_t(kTcGroupRows >> 3) << 17) | (uint32_t(kTcThreads >> 4) << 24);
-  u64 *dst = a.dst + blockIdx.z * a.dst_poly_stride;
+  const uint32_t tiles = uint32_t(n / kTcThreads);
   bool ok = true;
-  for (int g = 0; g < a.groups; ++g) {
-    if (tid == 0) {
-      for (int i = 0; i < kpad / 32; ++i) {
-        const u64 da = tc_desc(smem_addr(sa) + i * 2 * (kTcThreads / 8) * 128, (kTcThreads / 8) * 128, 128);
-        const u64 db = tc_desc(smem_addr(sb + g * kTcGroupRows * kpad) + i * 2 * (kTcGroupRows / 8) * 128,
-                               (kTcGroupRows / 8) * 128, 128);
-        const uint32_t acc = i > 0;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-            "l"(da), "l"(db), "r"(idesc), "r"(acc));
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_addr(&mbar)));
+  uint32_t phase = 0;  // completed MMA groups so far (mbarrier phase parity)
+  for (int ti = 0; ti < kTcTilesPerCta && ok; ++ti) {
+    const uint32_t tile = blockIdx.x * kTcTilesPerCta + ti;
+    if (tile >= tiles) break;  // uniform across the CTA
+    const u64 k = u64(tile) * kTcThreads + tid;
+    // A row of this thread's coefficient: the byte limbs of y_j, zero-padded.
+    for (int j = 0; j < kpad / 8; ++j) {
+      const u64 y = j < s ? shoup_canon(src[u64(j) * n + k], sinv[j].w, sinv[j].wq, sq[j]) : 0;
+      *reinterpret_cast<u64 *>(sa + tc_canon(tid, j * 8, kTcThreads)) = y;  // little-endian bytes = limbs
     }
-    uint32_t done = 0;
-    for (int it = 0; it < (1 << 20) && !done; ++it)
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-          "selp.u32 %0, 1, 0, p;\n\t}\n"
-          : "=r"(done)
-          : "r"(smem_addr(&mbar)), "r"(uint32_t(g & 1)));
-    // One decision for the whole CTA: every thread leaves together on a timeout.
-    const bool all_done = __syncthreads_and(done != 0);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (!all_done) {
-      ok = false;
-      break;
-    }
-    const int tl_end = min(kTcGroupTargets, t_count - g * kTcGroupTargets);
-    // Four targets' 8 columns per load, one wait per load.
-    for (int tq = 0; tq < kTcGroupTargets; tq += 4) {
-      if (tq >= tl_end) break;
-      uint32_t v[32];
-      const uint32_t addr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(tq * 8);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-          : "r"(addr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;");
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int tl = tq + u;
-        if (tl >= tl_end) break;
-        const uint32_t *w = v + 8 * u;
-        const u64 lo4 = u64(w[0]) + (u64(w[1]) << 8) + (u64(w[2]) << 16) + (u64(w[3]) << 24);
-        const u64 hi4 = u64(w[4]) + (u64(w[5]) << 8) + (u64(w[6]) << 16) + (u64(w[7]) << 24);
-        const int t = g * kTcGroupTargets + tl;
-        const u64 m = tm[t];
-        // hi4 * 2^32 mod m in [0, 4m) (w = 2^32 < m), plus lo4 < 2^47 <= m: below 5m.
-        u64 r = shoup_approx(hi4, u64(1) << 32, twq[t], 0 - m) + lo4;
-        r = csub_sign(r, 4 * m);  // [0, 4m)
-        if constexpr (!LAZY_OUT) r = csub_sign(csub_sign(r, 2 * m), m);
-        dst[u64(a.slot[t]) * n + k] = r;
-      }
-    }
-    // Every lane's loads are done before the next group's MMA reuses the columns.
+    asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ti == 0) {  // B must have landed before the first MMA reads it
+      uint32_t got = 0;
+      for (int it = 0; it < (1 << 20) && !got; ++it)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(got)
+            : "r"(smem_addr(&bbar)), "r"(0u));
+      if (!__syncthreads_and(got != 0)) {
+        ok = false;
+        break;
+      }
+    }
+    for (int g = 0; g < a.groups; ++g) {
+      if (tid == 0) {
+        for (int i = 0; i < kpad / 32; ++i) {
+          const u64 da = tc_desc(smem_addr(sa) + i * 2 * (kTcThreads / 8) * 128, (kTcThreads / 8) * 128, 128);
+          const u64 db = tc_desc(smem_addr(sb + g * kTcGroupRows * kpad) + i * 2 * (kTcGroupRows / 8) * 128,
+                                 (kTcGroupRows / 8) * 128, 128);
+          const uint32_t acc = i > 0;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+              "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_addr(&mbar)));
+      }
+      uint32_t done = 0;
+      for (int it = 0; it < (1 << 20) && !done; ++it)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_addr(&mbar)), "r"(phase & 1));
+      ++phase;
+      // One decision for the whole CTA: every thread leaves together on a timeout.
+      const bool all_done = __syncthreads_and(done != 0);
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      if (!all_done) {
+        ok = false;
+        break;
+      }
+      const int tl_end = min(kTcGroupTargets, t_count - g * kTcGroupTargets);
+      // Four targets' 8 columns per load, one wait per load.
+      for (int tq = 0; tq < kTcGroupTargets; tq += 4) {
+        if (tq >= tl_end) break;
+        uint32_t v[32];
+        const uint32_t addr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(tq * 8);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(addr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int tl = tq + u;
+          if (tl >= tl_end) break;
+          const uint32_t *w = v + 8 * u;
+          const u64 lo4 = u64(w[0]) + (u64(w[1]) << 8) + (u64(w[2]) << 16) + (u64(w[3]) << 24);
+          const u64 hi4 = u64(w[4]) + (u64(w[5]) << 8) + (u64(w[6]) << 16) + (u64(w[7]) << 24);
+          const int t = g * kTcGroupTargets + tl;
+          const u64 m = tm[t];
+          // hi4 * 2^32 mod m in [0, 4m) (w = 2^32 < m), plus lo4 < 2^47 <= m: below 5m.
+          u64 r = shoup_approx(hi4, u64(1) << 32, twq[t], 0 - m) + lo4;
+          r = csub_sign(r, 4 * m);  // [0, 4m)
+          if constexpr (!LAZY_OUT) r = csub_sign(csub_sign(r, 2 * m), m);
+          dst[u64(a.slot[t]) * n + k] = r;
+        }
+      }
+      // Every lane's loads are done before the next MMA reuses the columns.
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;");
+    }
   }
-  if (!ok) atomicExch(a.err, 1);
+  if (!ok && tid == 0) atomicExch(a.err, 1);
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcGroupRows));
