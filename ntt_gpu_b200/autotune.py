@@ -80,30 +80,39 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         kctx.keyswitch_batch(24, batch, ob, oa, xs, kb, ka, ws)
 
     passes = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col")
-    # tunable -> (candidates, workload, kernel classes whose device time decides it)
+    # tunable -> (candidates, workload, kernel classes whose device time decides it, tunables pinned
+    # while it is measured). The CUDA-core conversion choices serve the plans the tensor-core form
+    # does not take (more than 16 sources, moduli outside [2^48, 2^61)), so they are measured with it off.
+    cuda_core_conv = {"conv_tc": 0}
     plan = [
-        ("ntt_persistent", (0, 1), ntt_step, passes),
-        ("ntt_minb_fwd_col", (3, 4), ntt_step, ("ntt_fwd_col",)),
-        ("ntt_minb_fwd_row", (3, 4), ntt_step, ("ntt_fwd_row",)),
-        ("ntt_minb_inv_row", (3, 4), ntt_step, ("ntt_inv_row",)),
-        ("ntt_minb_inv_col", (3, 4), ntt_step, ("ntt_inv_col",)),
-        ("ntt_stage_tw_fwd_row", (0, 1), ntt_step, ("ntt_fwd_row",)),
-        ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",)),
-        ("conv_limbs", (0, 1), ks_step, ("conv",)),
-        ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",)),
-        ("mac_limbs", (0, 1), ks_step, ("mac",)),
-        ("conv_tc", (0, 1), ks_step, ("conv",)),
+        ("ntt_persistent", (0, 1), ntt_step, passes, {}),
+        ("ntt_minb_fwd_col", (3, 4), ntt_step, ("ntt_fwd_col",), {}),
+        ("ntt_minb_fwd_row", (3, 4), ntt_step, ("ntt_fwd_row",), {}),
+        ("ntt_minb_inv_row", (3, 4), ntt_step, ("ntt_inv_row",), {}),
+        ("ntt_minb_inv_col", (3, 4), ntt_step, ("ntt_inv_col",), {}),
+        ("ntt_stage_tw_fwd_row", (0, 1), ntt_step, ("ntt_fwd_row",), {}),
+        ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",), {}),
+        ("conv_limbs", (0, 1), ks_step, ("conv",), cuda_core_conv),
+        ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",), cuda_core_conv),
+        ("mac_limbs", (0, 1), ks_step, ("mac",), {}),
+        ("conv_tc", (0, 1), ks_step, ("conv",), {}),
     ]
     measurements, choices = {}, {}
-    for name, candidates, step, kernels in plan:
+    for name, candidates, step, kernels, pinned in plan:
+        saved = {k: nb.tuning_get(k) for k in pinned}
+        for k, v in pinned.items():
+            nb.tuning_set(k, v)
         times = {}
         for value in candidates:
             nb.tuning_set(name, value)
             times[value] = sum(_device_ms(nb, torch, step, iters, kernels).values())
         best = min(times, key=times.get)
         nb.tuning_set(name, best)
+        for k, v in saved.items():
+            nb.tuning_set(k, v)
         choices[name] = best
-        measurements[name] = {"measured_by": list(kernels), "device_ms_per_call": {str(k): v for k, v in times.items()}}
+        measurements[name] = {"measured_by": list(kernels), "pinned": dict(pinned),
+                              "device_ms_per_call": {str(k): v for k, v in times.items()}}
 
     def total(step):
         torch.cuda.synchronize()
