@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-vs-plain Poisson legs")
+    ap.add_argument("--tune", action="append", default=[], metavar="NAME=VALUE",
+                    help="profiling: override a launch tunable (repeatable), e.g. --tune conv_tc=0")
     ap.add_argument("--rotate", action="store_true",
                     help="profiling: every batched request also adds P*c0 and rotates by g = 5 (rotate kernel)")
     ap.add_argument("--kernels-only", action="store_true",
@@ -474,6 +476,9 @@ def run_ours(args, rank, world, local):
 
     device = local
     torch.cuda.set_device(device)
+    for item in args.tune:
+        name, value = item.split("=", 1)
+        nb.tuning_set(name, int(value))
     dev = torch.device(f"cuda:{device}")
     B = args.batch
     prm = synthetic_params(N, LEVEL, K_P, DNUM)
