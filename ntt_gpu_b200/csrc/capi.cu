@@ -111,6 +111,21 @@ uint32_t h_bitrev(uint32_t x, int bits) {
   for (int i = 0; i < bits; ++i) r = (r << 1) | ((x >> i) & 1);
   return r;
 }
+// Reorders one tower's twiddle table (bit-reversed group layout) into the
+// row passes' lane-major order for stages logN-4 .. logN-1 (b200::row_lane_major).
+void lane_major_rows(ulonglong2 *tw, int logn) {
+  const int lr = logn - 8;
+  std::vector<ulonglong2> block;
+  for (int sp = 4; sp < 8; ++sp) {
+    const uint32_t s = lr + sp, width = 1u << sp, lanes_k = 1u << (sp - 4);
+    for (uint32_t row = 0; row < (1u << lr); ++row) {
+      ulonglong2 *b = tw + (1u << s) + row * width;
+      block.assign(b, b + width);
+      for (uint32_t u = 0; u < 16; ++u)
+        for (uint32_t k = 0; k < lanes_k; ++k) b[b200::row_lane_major(u, k)] = block[u * lanes_k + k];
+    }
+  }
+}
 b200::Reducer h_reducer(u64 m) {
   b200::Reducer r;
   r.m = m;
@@ -396,6 +411,7 @@ Tunable g_tuning[] = {
     {"ntt_minb_fwd_row", {4}, 3, 4},
     {"ntt_minb_inv_row", {4}, 3, 4},
     {"ntt_minb_inv_col", {4}, 3, 4},
+    {"ntt_col_direct", {0}, 0, 1},     // column passes load and store between registers and global memory
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
@@ -494,7 +510,10 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
   } while (0)
   if (!inverse) {
     Timed t1("ntt_fwd_col", st);
-    NTT_LAUNCH(fwd_col, b);
+    if (tuned("ntt_col_direct"))
+      NTT_LAUNCH(fwd_col, b, true);
+    else
+      NTT_LAUNCH(fwd_col, b, false);
     t1.done();
     Timed t2("ntt_fwd_row", st);
     if (tuned("ntt_stage_tw_fwd_row"))
@@ -510,7 +529,10 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
       NTT_LAUNCH(inv_row, b, false);
     t1.done();
     Timed t2("ntt_inv_col", st);
-    NTT_LAUNCH(inv_col, second);
+    if (tuned("ntt_col_direct"))
+      NTT_LAUNCH(inv_col, second, true);
+    else
+      NTT_LAUNCH(inv_col, second, false);
     t2.done();
   }
 #undef NTT_LAUNCH
@@ -1213,6 +1235,7 @@ int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const
           const uint32_t idx = h_bitrev((uint32_t)e, c->logn);
           dst[idx] = make_ulonglong2(w, h_shoup(w, mq));
         }
+        if (c->logn >= b200::kLaneMajorMinLogn) lane_major_rows(dst, c->logn);
       }
       const u64 ninv = h_inv(n % mq, mq);
       tc[g].q = mq;

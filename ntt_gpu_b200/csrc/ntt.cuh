@@ -94,6 +94,31 @@ __device__ __forceinline__ TowerView tower_view(const NttBatch &b, const DeviceT
   return v;
 }
 
+// Block indices passed through an empty asm, so that addresses recomputed from
+// them at the end of a kernel are not merged with the copies computed at its
+// start (which would keep those alive, in registers or spilled, across the
+// butterflies).
+struct BlockIds {
+  uint32_t x, y, z;
+};
+__device__ __forceinline__ BlockIds fresh_block_ids() {
+  BlockIds i{blockIdx.x, blockIdx.y, blockIdx.z};
+  asm volatile("" : "+r"(i.x), "+r"(i.y), "+r"(i.z));
+  return i;
+}
+// Offset of slot i.y's tower inside a polynomial, and that tower's destination.
+__device__ __forceinline__ u64 tower_offset(const NttBatch &b, const DeviceTables &T, const BlockIds &i) {
+  return u64(b.off[i.y]) * (u64(1) << T.logn);
+}
+__device__ __forceinline__ u64 *tower_dst(const NttBatch &b, const DeviceTables &T, const BlockIds &i) {
+  return poly_dst(b, i.z) + tower_offset(b, T, i);
+}
+
+// Hint: bring [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ Shoup tw_load(const ulonglong2 *p) {
   const ulonglong2 v = __ldg(p);
   return Shoup{v.x, v.y};
@@ -149,22 +174,34 @@ struct ColGeom {
   }
 };
 
-template <int LOGN, int MODE, int MINB>
+// DIRECT: the half-warps of both mappings read and write 16 or more
+// consecutive words of one row, so with DIRECT set the passes load their
+// inputs and store their outputs straight between registers and global memory
+// (coalesced 8-byte accesses) and use shared memory only for the exchange
+// between the two register phases.
+template <int LOGN, int MODE, int MINB, bool DIRECT>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
+  constexpr u64 kStride = N >> G::LR;
   __shared__ __align__(16) u64 tile[kTileWords];
   __shared__ ulonglong2 tw[G::R];
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
-  for (int i = threadIdx.x; i < G::R; i += kNttThreads) tw[i] = v.tw[i];
   const int col0 = blockIdx.x * G::COLS;
-  load_block<G::R, G::COLS, G::COLS, false>(tile, v.src + col0, N >> G::LR);
-  __syncthreads();
   const int c = threadIdx.x % G::COLS, u = threadIdx.x / G::COLS;
   u64 x[16];
+  if constexpr (DIRECT) {
 #pragma unroll
-  for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+    for (int e = 0; e < 16; ++e) x[e] = v.src[G::row_a(e, u) * kStride + col0 + c];
+  }
+  for (int i = threadIdx.x; i < G::R; i += kNttThreads) tw[i] = v.tw[i];
+  if constexpr (!DIRECT) load_block<G::R, G::COLS, G::COLS, false>(tile, v.src + col0, kStride);
+  __syncthreads();
+  if constexpr (!DIRECT) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+  }
   // Stages 0..3: row bit logR-1-s == register bit 3-s; group = e >> (4-s).
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
@@ -177,7 +214,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
     }
   }
   if constexpr (G::LR > 4) {
-    __syncthreads();
+    if constexpr (!DIRECT) __syncthreads();  // every thread has read its inputs from the tile
 #pragma unroll
     for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
     __syncthreads();
@@ -194,35 +231,57 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
         ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
       }
     }
+    if constexpr (DIRECT) {
+#pragma unroll
+      u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) dst[G::row_b(e, u) * kStride] = x[e];
+      return;
+    }
     __syncthreads();
 #pragma unroll
     for (int e = 0; e < 16; ++e) tile[G::row_b(e, u) * G::COLS + c] = x[e];
   } else {
+    if constexpr (DIRECT) {
+#pragma unroll
+      u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) dst[G::row_a(e, u) * kStride] = x[e];
+      return;
+    }
     __syncthreads();
 #pragma unroll
     for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
   }
   __syncthreads();
-  store_block<G::R, G::COLS, G::COLS, false>(v.dst + col0, tile, N >> G::LR);
+  store_block<G::R, G::COLS, G::COLS, false>(tower_dst(b, T, fresh_block_ids()) + col0, tile, kStride);
 }
 
-template <int LOGN, int MODE, int MINB>
+template <int LOGN, int MODE, int MINB, bool DIRECT>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
+  constexpr u64 kStride = N >> G::LR;
   __shared__ __align__(16) u64 tile[kTileWords];
   __shared__ ulonglong2 tw[G::R];
   const TowerView v = tower_view(b, T, true);
   const u64 q = v.c->q, q2 = v.c->q2;
-  for (int i = threadIdx.x; i < G::R; i += kNttThreads) tw[i] = v.tw[i];
   const int col0 = blockIdx.x * G::COLS;
-  load_block<G::R, G::COLS, G::COLS, false>(tile, v.src + col0, N >> G::LR);
-  __syncthreads();
   const int c = threadIdx.x % G::COLS, u = threadIdx.x / G::COLS;
   u64 x[16];
-  if constexpr (G::LR > 4) {
+  if constexpr (DIRECT) {
 #pragma unroll
-    for (int e = 0; e < 16; ++e) x[e] = tile[G::row_b(e, u) * G::COLS + c];
+    for (int e = 0; e < 16; ++e)
+      x[e] = v.src[(G::LR > 4 ? G::row_b(e, u) : G::row_a(e, u)) * kStride + col0 + c];
+  }
+  for (int i = threadIdx.x; i < G::R; i += kNttThreads) tw[i] = v.tw[i];
+  if constexpr (!DIRECT) load_block<G::R, G::COLS, G::COLS, false>(tile, v.src + col0, kStride);
+  __syncthreads();
+  if constexpr (G::LR > 4) {
+    if constexpr (!DIRECT) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) x[e] = tile[G::row_b(e, u) * G::COLS + c];
+    }
     // Stages logR-1 .. 4: row bit logR-1-s == register bit logR-1-s.
 #pragma unroll
     for (int s = G::LR - 1; s >= 4; --s) {
@@ -234,13 +293,16 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
         gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
       }
     }
-    __syncthreads();
+    if constexpr (!DIRECT) __syncthreads();  // every thread has read its inputs from the tile
 #pragma unroll
     for (int e = 0; e < 16; ++e) tile[G::row_b(e, u) * G::COLS + c] = x[e];
     __syncthreads();
-  }
 #pragma unroll
-  for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+    for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+  } else if constexpr (!DIRECT) {
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
+  }
   // Stages 3..1, then stage 0 with N^-1 folded in.
 #pragma unroll
   for (int s = 3; s >= 1; --s) {
@@ -255,11 +317,18 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
   const Shoup ninv = v.c->ninv, last = v.c->last_inv;
 #pragma unroll
   for (int e = 0; e < 8; ++e) gs_last<MODE>(x[e], x[e + 8], ninv, last, q, q2);
+  if constexpr (DIRECT) {
+#pragma unroll
+    u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) dst[G::row_a(e, u) * kStride] = x[e];
+    return;
+  }
   __syncthreads();
 #pragma unroll
   for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
   __syncthreads();
-  store_block<G::R, G::COLS, G::COLS, false>(v.dst + col0, tile, N >> G::LR);
+  store_block<G::R, G::COLS, G::COLS, false>(tower_dst(b, T, fresh_block_ids()) + col0, tile, kStride);
 }
 
 // ---- row pass ----------------------------------------------------------------
@@ -294,12 +363,12 @@ __device__ __forceinline__ void store_rows_warp(u64 *g, const u64 *tile) {
   }
 }
 
-// Twiddle staging for the row passes' register-bit stages (s' = 4..7, where
-// lane u of row r needs T[2^s + (row << s') + ((16u + e) >> (8 - s'))]): with STW
-// set, the CTA first copies the stage's 16 * 2^s' twiddles, contiguous in the
-// table, into shared memory with coalesced 16-byte loads, entry k at 16-byte
-// slot k + k/8. The pad keeps the eight lanes of every quarter-warp on distinct
-// bank groups for all four stages, and the data tile's buffer (free while the
+// Twiddles of the row passes' register-bit stages (s' = 4..7): lane u of row r
+// needs T[2^s + (row << s') + (16u + e) >> (8 - s')], which the tables hold in
+// lane-major order (row_lane_major), so the 16 lanes of a row read 16
+// consecutive entries. With STW set, the CTA first copies the stage's 16 * 2^s'
+// twiddles, contiguous in the table, into shared memory with coalesced 16-byte
+// loads, entry k at 16-byte slot k + k/8; the data tile's buffer (free while the
 // values sit in registers) holds the largest stage (2048 entries, 36 KiB).
 constexpr int kRowStwWords = 2 * (2048 + 2048 / 8);
 __device__ __forceinline__ void stage_twiddles(ulonglong2 *st, const ulonglong2 *tw, int s, int sp, int row0) {
@@ -319,6 +388,14 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
+  if (b.epi_left != nullptr && (threadIdx.x & 31) == 0) {
+    // The ModDown epilogue reads its operands only after the butterflies:
+    // start moving this warp's two rows of them (4 KiB per operand) into L2 now.
+    const u64 off = u64(b.off[blockIdx.y]) * (u64(1) << T.logn) + (row0 + 2 * (threadIdx.x >> 5)) * 256;
+    prefetch_l2(b.epi_left + blockIdx.z * b.epi_left_stride + off, 2 * 256 * sizeof(u64));
+    const u64 *add = poly_add(b, blockIdx.z);
+    if (add) prefetch_l2(add + off, 2 * 256 * sizeof(u64));
+  }
   if constexpr (STW) {
     load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
     __syncthreads();
@@ -361,7 +438,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
-        const Shoup w = staged_twiddle(st, (r << sp) + ((u * 16 + e) >> (8 - sp)));
+        const Shoup w = staged_twiddle(st, (r << sp) + row_lane_major(u, e >> (8 - sp)));
         ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
@@ -373,7 +450,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
-        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
         ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
@@ -388,19 +465,20 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   } else {
     __syncwarp();
   }
+  const BlockIds ids = fresh_block_ids();
+  const u64 rows_off = tower_offset(b, T, ids) + ids.x * 16 * 256;
+  u64 *out = poly_dst(b, ids.z) + rows_off;
   if (b.epi_left == nullptr) {
     if constexpr (STW)
-      store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+      store_block<16, 256, kRowPad, true>(out, tile, 256);
     else
-      store_rows_warp(v.dst + row0 * 256, tile);
+      store_rows_warp(out, tile);
     return;
   }
-  const u64 *left = b.epi_left + blockIdx.z * b.epi_left_stride + u64(b.off[blockIdx.y]) * (u64(1) << T.logn) +
-                    row0 * 256;
-  const Shoup pinv = b.epi_pinv[b.id[blockIdx.y]];
-  u64 *out = v.dst + row0 * 256;
-  const u64 *add = poly_add(b, blockIdx.z);
-  if (add) add += u64(b.off[blockIdx.y]) * (u64(1) << T.logn) + row0 * 256;
+  const u64 *left = b.epi_left + ids.z * b.epi_left_stride + rows_off;
+  const Shoup pinv = b.epi_pinv[b.id[ids.y]];
+  const u64 *add = poly_add(b, ids.z);
+  if (add) add += rows_off;
   // Epilogue over the rows this thread's group owns: every row with STW (the
   // CTA synchronised above), the warp's own two rows otherwise.
   const int j0 = STW ? int(threadIdx.x) : int(threadIdx.x & 31) + (int(threadIdx.x >> 5) * 2) * 128;
@@ -454,7 +532,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
-        const Shoup w = staged_twiddle(st, (r << sp) + ((u * 16 + e) >> (8 - sp)));
+        const Shoup w = staged_twiddle(st, (r << sp) + row_lane_major(u, e >> (8 - sp)));
         gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
@@ -466,7 +544,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
-        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
         gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
@@ -492,10 +570,10 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
   for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
   if constexpr (STW) {
     __syncthreads();
-    store_block<16, 256, kRowPad, true>(v.dst + row0 * 256, tile, 256);
+    store_block<16, 256, kRowPad, true>(tower_dst(b, T, fresh_block_ids()) + row0 * 256, tile, 256);
   } else {
     __syncwarp();
-    store_rows_warp(v.dst + row0 * 256, tile);
+    store_rows_warp(tower_dst(b, T, fresh_block_ids()) + row0 * 256, tile);
   }
 }
 

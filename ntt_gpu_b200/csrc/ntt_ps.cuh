@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
-          const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+          const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
           ct_butterfly<MODE>(x[e], x[e + d], t.w, t.wq, q, q2);
         }
       }
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kNttThreads, 3) ntt_row_ps(NttBatch b, DeviceT
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
-          const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + ((u * 16 + e) >> (8 - sp)));
+          const Shoup t = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
           gs_butterfly<MODE>(x[e], x[e + d], t.w, t.wq, q, q2);
         }
       }

@@ -27,6 +27,16 @@ struct DeviceTables {
   int logn;
 };
 
+// Lane-major order of the row passes' register-bit stages. In a two-pass
+// transform (N >= 2^12, R = N / 256 rows, logR = logN - 8) stage s = logR + sp,
+// sp = 4..7, gives row `row` the 2^sp entries at 2^s + row * 2^sp, and lane u
+// (0..15) of that row reads offsets u * 2^(sp-4) + k, k < 2^(sp-4). The tables
+// hold offset u * 2^(sp-4) + k at position 16 k + u, so for a fixed k the 16
+// lanes of a row read 16 consecutive entries (256 contiguous bytes) instead of
+// entries 2^(sp-4) apart. Stages below logR + 4 keep the plain layout.
+__host__ __device__ constexpr uint32_t row_lane_major(uint32_t u, uint32_t k) { return (k << 4) | u; }
+constexpr int kLaneMajorMinLogn = 12;
+
 // Approximate-CRT switch from `s` source towers to `t` target towers
 // (include/ntt/basis_conversion.hpp:13-30):
 //   y_j = [x_j * Bhat_j^-1]_{b_j},  out_i = [sum_j y_j * [Bhat_j]_{m_i}]_{m_i}.
