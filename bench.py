@@ -44,7 +44,7 @@ WORKLOAD = ("batched Hybrid key switch: 16 ciphertext components per GPU at N=2^
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch", type=int, default=BATCH)
@@ -86,9 +86,15 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-i", str(self.device), "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
-            time.sleep(0.3)
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi can take a second to start: the timed region begins after its first sample.
+        deadline = time.time() + 10
+        while time.time() < deadline and self.proc.poll() is None:
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:

@@ -411,7 +411,8 @@ Tunable g_tuning[] = {
     {"ntt_minb_fwd_row", {4}, 3, 4},
     {"ntt_minb_inv_row", {4}, 3, 4},
     {"ntt_minb_inv_col", {4}, 3, 4},
-    {"ntt_col_direct", {0}, 0, 1},     // column passes load and store between registers and global memory
+    {"ntt_col_direct", {1}, 0, 1},     // column passes load and store between registers and global memory
+    {"ntt_row_direct", {1}, 0, 1},     // row passes load (forward) / store (inverse) mapping A directly
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
@@ -467,7 +468,7 @@ void launch_row_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32
 template <int LOGN, int MODE>
 void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
                       bool inverse, cudaStream_t st) {
-  const dim3 grid((1u << LOGN) / b200::kTileWords, slots, polys);
+  const dim3 grid((1u << LOGN) / b200::kTileWords, polys, slots);
   b200::NttBatch second = b;
   second.src = b.dst;
   second.src_stride = b.dst_stride;
@@ -517,16 +518,20 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     t1.done();
     Timed t2("ntt_fwd_row", st);
     if (tuned("ntt_stage_tw_fwd_row"))
-      NTT_LAUNCH(fwd_row, second, true);
+      NTT_LAUNCH(fwd_row, second, true, false);
+    else if (tuned("ntt_row_direct"))
+      NTT_LAUNCH(fwd_row, second, false, true);
     else
-      NTT_LAUNCH(fwd_row, second, false);
+      NTT_LAUNCH(fwd_row, second, false, false);
     t2.done();
   } else {
     Timed t1("ntt_inv_row", st);
     if (tuned("ntt_stage_tw_inv_row"))
-      NTT_LAUNCH(inv_row, b, true);
+      NTT_LAUNCH(inv_row, b, true, false);
+    else if (tuned("ntt_row_direct"))
+      NTT_LAUNCH(inv_row, b, false, true);
     else
-      NTT_LAUNCH(inv_row, b, false);
+      NTT_LAUNCH(inv_row, b, false, false);
     t1.done();
     Timed t2("ntt_inv_col", st);
     if (tuned("ntt_col_direct"))
@@ -561,11 +566,17 @@ dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
 // (forward only) redirects the final pass: split destination and/or the ModDown
 // epilogue (left - x) * P^-1; small transforms run it as a separate kernel.
 // src_list (device array, one entry per polynomial) replaces src / src_stride.
-void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots, size_t polys,
+void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots_in, size_t polys,
              u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr,
              const u64 *const *src_list = nullptr) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   require(!fin || !inverse, "final-pass redirection is forward only");
+  // Slots of one tower (e.g. the same target tower of several Hybrid digits)
+  // run back to back, so its twiddle table is read from HBM once per launch.
+  // Every slot carries its own offset and tower id, so the order changes no
+  // result; ascending Q-slot layouts keep their order.
+  std::vector<Slot> slots(slots_in);
+  std::stable_sort(slots.begin(), slots.end(), [](const Slot &a, const Slot &b) { return a.id < b.id; });
   for (size_t first = 0; first < slots.size(); first += b200::kMaxSlots) {
     const size_t count = std::min<size_t>(b200::kMaxSlots, slots.size() - first);
     b200::NttBatch b{};
@@ -579,7 +590,7 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
     b.dst = dst;
     b.src_list = src_list;
     if (c.logn <= 11) {
-      const dim3 grid(1, (unsigned)count, (unsigned)polys);
+      const dim3 grid(1, (unsigned)polys, (unsigned)count);
       const int threads = std::min<int>(b200::kNttThreads, std::max<int>(32, (int)(c.n / 2)));
       {
         Timed t("ntt_small", st);

@@ -30,9 +30,11 @@ constexpr int kNttThreads = 256;
 constexpr int kTileWords = 4096;
 constexpr int kRowPad = 272;  // 256 words + one pad word per 16
 
-// A batch of tower transforms: slot y (blockIdx.y) of polynomial z
-// (blockIdx.z) is read at src + z * src_stride + off[y] * N, written at
+// A batch of tower transforms: slot y (blockIdx.z) of polynomial z
+// (blockIdx.y) is read at src + z * src_stride + off[y] * N, written at
 // dst + z * dst_stride + off[y] * N, and uses the tables of global tower id[y].
+// Polynomials vary faster than slots, so the CTAs that read one tower's
+// twiddle table run back to back and find it in L2.
 // Optional destination split: with dst_odd set, polynomial z is written at
 // (z odd ? dst_odd : dst) + (z / 2) * dst_stride (the b and a channels of a
 // key switch land in separate caller buffers).
@@ -81,14 +83,14 @@ struct TowerView {
 };
 
 __device__ __forceinline__ TowerView tower_view(const NttBatch &b, const DeviceTables &T, bool inv) {
-  const uint32_t slot = blockIdx.y;
+  const uint32_t slot = blockIdx.z;
   const uint32_t g = b.id[slot];
   const u64 n = u64(1) << T.logn;
   const u64 offset = u64(b.off[slot]) * n;
   TowerView v;
   v.c = T.tc + g;
   v.tw = (inv ? T.inv : T.fwd) + g * n;
-  const u64 z = blockIdx.z;
+  const u64 z = blockIdx.y;
   v.src = poly_src(b, z) + offset;
   v.dst = poly_dst(b, z) + offset;
   return v;
@@ -99,19 +101,19 @@ __device__ __forceinline__ TowerView tower_view(const NttBatch &b, const DeviceT
 // start (which would keep those alive, in registers or spilled, across the
 // butterflies).
 struct BlockIds {
-  uint32_t x, y, z;
+  uint32_t x, slot, poly;
 };
 __device__ __forceinline__ BlockIds fresh_block_ids() {
-  BlockIds i{blockIdx.x, blockIdx.y, blockIdx.z};
-  asm volatile("" : "+r"(i.x), "+r"(i.y), "+r"(i.z));
+  BlockIds i{blockIdx.x, blockIdx.z, blockIdx.y};
+  asm volatile("" : "+r"(i.x), "+r"(i.slot), "+r"(i.poly));
   return i;
 }
-// Offset of slot i.y's tower inside a polynomial, and that tower's destination.
+// Offset of the slot's tower inside a polynomial, and that tower's destination.
 __device__ __forceinline__ u64 tower_offset(const NttBatch &b, const DeviceTables &T, const BlockIds &i) {
-  return u64(b.off[i.y]) * (u64(1) << T.logn);
+  return u64(b.off[i.slot]) * (u64(1) << T.logn);
 }
 __device__ __forceinline__ u64 *tower_dst(const NttBatch &b, const DeviceTables &T, const BlockIds &i) {
-  return poly_dst(b, i.z) + tower_offset(b, T, i);
+  return poly_dst(b, i.poly) + tower_offset(b, T, i);
 }
 
 // Hint: bring [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
@@ -381,8 +383,14 @@ __device__ __forceinline__ Shoup staged_twiddle(const ulonglong2 *st, int k) {
   return Shoup{v.x, v.y};
 }
 
-template <int LOGN, int MODE, int MINB, bool STW>
+// DIRECT (without STW): in mapping A the 16 lanes of a row read 16
+// consecutive words, so the forward row pass loads its inputs, and the inverse
+// row pass stores its outputs, straight between registers and global memory;
+// the other side stays staged through the warp's tile rows (mapping B puts the
+// lanes 128 bytes apart).
+template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
+  static_assert(!(STW && DIRECT), "the staged-twiddle form has no direct variant");
   constexpr int LR = LOGN - 8;
   __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
   const TowerView v = tower_view(b, T, false);
@@ -391,24 +399,30 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   if (b.epi_left != nullptr && (threadIdx.x & 31) == 0) {
     // The ModDown epilogue reads its operands only after the butterflies:
     // start moving this warp's two rows of them (4 KiB per operand) into L2 now.
-    const u64 off = u64(b.off[blockIdx.y]) * (u64(1) << T.logn) + (row0 + 2 * (threadIdx.x >> 5)) * 256;
-    prefetch_l2(b.epi_left + blockIdx.z * b.epi_left_stride + off, 2 * 256 * sizeof(u64));
-    const u64 *add = poly_add(b, blockIdx.z);
+    const u64 off = u64(b.off[blockIdx.z]) * (u64(1) << T.logn) + (row0 + 2 * (threadIdx.x >> 5)) * 256;
+    prefetch_l2(b.epi_left + blockIdx.y * b.epi_left_stride + off, 2 * 256 * sizeof(u64));
+    const u64 *add = poly_add(b, blockIdx.y);
     if (add) prefetch_l2(add + off, 2 * 256 * sizeof(u64));
-  }
-  if constexpr (STW) {
-    load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
-    __syncthreads();
-  } else {
-    load_rows_warp(tile, v.src + row0 * 256);
-    __syncwarp();
   }
   const int r = threadIdx.x / 16, u = threadIdx.x % 16;
   const int row = row0 + r;
   u64 *my = tile + r * kRowPad;
   u64 x[16];
+  if constexpr (DIRECT) {
+    const u64 *in = v.src + row * 256 + u;
 #pragma unroll
-  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+    for (int e = 0; e < 16; ++e) x[e] = in[e * 16];
+  } else {
+    if constexpr (STW) {
+      load_block<16, 256, kRowPad, true>(tile, v.src + row0 * 256, 256);
+      __syncthreads();
+    } else {
+      load_rows_warp(tile, v.src + row0 * 256);
+      __syncwarp();
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+  }
   // Stages LR + s', s' = 0..3: column bit 7-s' == register bit 3-s'.
 #pragma unroll
   for (int sp = 0; sp < 4; ++sp) {
@@ -467,7 +481,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   }
   const BlockIds ids = fresh_block_ids();
   const u64 rows_off = tower_offset(b, T, ids) + ids.x * 16 * 256;
-  u64 *out = poly_dst(b, ids.z) + rows_off;
+  u64 *out = poly_dst(b, ids.poly) + rows_off;
   if (b.epi_left == nullptr) {
     if constexpr (STW)
       store_block<16, 256, kRowPad, true>(out, tile, 256);
@@ -475,9 +489,9 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
       store_rows_warp(out, tile);
     return;
   }
-  const u64 *left = b.epi_left + ids.z * b.epi_left_stride + rows_off;
-  const Shoup pinv = b.epi_pinv[b.id[ids.y]];
-  const u64 *add = poly_add(b, ids.z);
+  const u64 *left = b.epi_left + ids.poly * b.epi_left_stride + rows_off;
+  const Shoup pinv = b.epi_pinv[b.id[ids.slot]];
+  const u64 *add = poly_add(b, ids.poly);
   if (add) add += rows_off;
   // Epilogue over the rows this thread's group owns: every row with STW (the
   // CTA synchronised above), the warp's own two rows otherwise.
@@ -500,8 +514,9 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   }
 }
 
-template <int LOGN, int MODE, int MINB, bool STW>
+template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
+  static_assert(!(STW && DIRECT), "the staged-twiddle form has no direct variant");
   constexpr int LR = LOGN - 8;
   __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
   const TowerView v = tower_view(b, T, true);
@@ -565,6 +580,12 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
       const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
       gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
     }
+  }
+  if constexpr (DIRECT) {
+    u64 *const out = tower_dst(b, T, fresh_block_ids()) + row * 256 + u;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) out[e * 16] = x[e];
+    return;
   }
 #pragma unroll
   for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
