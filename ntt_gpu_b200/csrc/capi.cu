@@ -419,6 +419,7 @@ Tunable g_tuning[] = {
     {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
     {"conv_tc", {1}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
+    {"conv_tc_tiles", {4}, 1, 16},     // 128-coefficient tiles per tensor-core conversion CTA
 };
 Tunable *find_tunable(const char *name) {
   for (auto &t : g_tuning)
@@ -690,7 +691,9 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
       attr_set[c.device][which] = 1;
     }
     const size_t tiles = c.n / b200::kTcThreads;
-    const dim3 grid((unsigned)((tiles + b200::kTcTilesPerCta - 1) / b200::kTcTilesPerCta), 1, (unsigned)polys);
+    const size_t per_cta = (size_t)tuned("conv_tc_tiles");
+    a.tiles_per_cta = (int)per_cta;
+    const dim3 grid((unsigned)((tiles + per_cta - 1) / per_cta), 1, (unsigned)polys);
     Timed t("conv", st);
     kernel<<<grid, b200::kTcThreads, smem, st>>>(a);
     t.done();

@@ -171,10 +171,10 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 // below 2^23): one [128 coefficients x 8s] x [8s x 8 per target] unsigned int8
 // matrix product with int32 accumulators in tensor memory. Each thread folds
 // its coefficient's eight S_tb per target into H * 2^32 + L (H, L < 2^47) and
-// reduces with one approximate-quotient Shoup product, (H * 2^32 mod m_t) in
-// [0, 4m) plus L, below 5m when 2^48 <= m_t < 2^61; the result is then brought
-// to [0, 4m) (lazy output) or to [0, m). It is congruent to conv_kernel's
-// output modulo m_t, hence identical once canonical.
+// reduces it with one approximate quotient (tc_fold_reduce) into [0, 3.5m) for
+// 2^48 <= m_t < 2^61; the result is left there (lazy output, within [0, 4m))
+// or brought to [0, m). It is congruent to conv_kernel's output modulo m_t,
+// hence identical once canonical.
 //
 // CTA = 128 threads = 128 coefficients = the 128 TMEM lanes. A: one row of
 // 8s bytes per coefficient. B: groups of 8 targets (64 rows of 8s bytes),
@@ -186,7 +186,6 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 constexpr int kTcThreads = 128;
 constexpr int kTcGroupTargets = 8;
 constexpr int kTcGroupRows = 64;  // 8 targets x 8 output bytes
-constexpr int kTcTilesPerCta = 4;  // coefficient tiles per CTA (B, TMEM and barriers set up once)
 struct ConvTcArgs {
   const ConvPlan *plan;
   const uint8_t *bmat;  // [groups][64 rows x kpad] bytes, canonical layout
@@ -195,8 +194,27 @@ struct ConvTcArgs {
   u64 src_poly_stride, dst_poly_stride;
   uint16_t slot[kMaxConvTargets];
   int logn, kpad, groups;
+  int tiles_per_cta;  // coefficient tiles per CTA (B, TMEM and barriers set up once per CTA)
   int *err;
 };
+
+// r == h * 2^32 + l (mod m), r in [0, 3.5m), for h, l < 2^47, 2^48 <= m < 2^61
+// and wq = floor(2^96 / m) (< 2^48). The quotient estimate
+//   e = hh*wh + floor((hh*wl + hl*wh) / 2^32)    (h = hh:hl, wq = wh:wl)
+// drops only hl*wl / 2^64 < 1 and a fraction below 1 from h * wq / 2^64, and
+// h * wq / 2^64 is within h / 2^64 < 2^-17 of h * 2^32 / m; so e is the true
+// quotient floor(h * 2^32 / m) minus 0, 1 or 2, and h * 2^32 - e m lies in
+// [0, 3m). Adding l < 2^47 <= m / 2 keeps the result below 3.5m. As e < 2^32,
+// e * m mod 2^64 takes one wide and one low 32-bit product, and h * 2^32 mod
+// 2^64 is hl in the high word. mneg = 2^64 - m.
+__device__ __forceinline__ u64 tc_fold_reduce(u64 h, u64 l, u64 mneg, u64 wq) {
+  const uint32_t hl = uint32_t(h), hh = uint32_t(h >> 32);
+  const uint32_t wl = uint32_t(wq), wh = uint32_t(wq >> 32);
+  const u64 mid = u64(hh) * wl + u64(hl) * wh;      // < 2^49
+  const uint32_t e = hh * wh + uint32_t(mid >> 32);  // < 2^32
+  const u64 base = l + (u64(hl) << 32);              // h * 2^32 + l mod 2^64
+  return base + u64(e) * uint32_t(mneg) + (u64(e * uint32_t(mneg >> 32)) << 32);
+}
 
 __host__ __device__ __forceinline__ int tc_canon(int r, int k, int rows) {
   return ((k >> 4) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 15);
@@ -260,8 +278,8 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   const uint32_t tiles = uint32_t(n / kTcThreads);
   bool ok = true;
   uint32_t phase = 0;  // completed MMA groups so far (mbarrier phase parity)
-  for (int ti = 0; ti < kTcTilesPerCta && ok; ++ti) {
-    const uint32_t tile = blockIdx.x * kTcTilesPerCta + ti;
+  for (int ti = 0; ti < a.tiles_per_cta && ok; ++ti) {
+    const uint32_t tile = blockIdx.x * a.tiles_per_cta + ti;
     if (tile >= tiles) break;  // uniform across the CTA
     const u64 k = u64(tile) * kTcThreads + tid;
     // A row of this thread's coefficient: the byte limbs of y_j, zero-padded.
@@ -337,13 +355,12 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
           const int tl = tq + u;
           if (tl >= tl_end) break;
           const uint32_t *w = v + 8 * u;
-          const u64 lo4 = u64(w[0]) + (u64(w[1]) << 8) + (u64(w[2]) << 16) + (u64(w[3]) << 24);
-          const u64 hi4 = u64(w[4]) + (u64(w[5]) << 8) + (u64(w[6]) << 16) + (u64(w[7]) << 24);
+          // Each sum is below 2^23, so w0 + w1 * 2^8 and w2 + w3 * 2^8 fit in 32 bits.
+          const u64 lo4 = u64(w[0] + (w[1] << 8)) + (u64(w[2] + (w[3] << 8)) << 16);
+          const u64 hi4 = u64(w[4] + (w[5] << 8)) + (u64(w[6] + (w[7] << 8)) << 16);
           const int t = g * kTcGroupTargets + tl;
           const u64 m = tm[t];
-          // hi4 * 2^32 mod m in [0, 4m) (w = 2^32 < m), plus lo4 < 2^47 <= m: below 5m.
-          u64 r = shoup_approx(hi4, u64(1) << 32, twq[t], 0 - m) + lo4;
-          r = csub_sign(r, 4 * m);  // [0, 4m)
+          u64 r = tc_fold_reduce(hi4, lo4, 0 - m, twq[t]);  // [0, 3.5m)
           if constexpr (!LAZY_OUT) r = csub_sign(csub_sign(r, 2 * m), m);
           dst[u64(a.slot[t]) * n + k] = r;
         }
