@@ -683,7 +683,8 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   a.kpad = p.tc_kpad;
   a.groups = p.tc_groups;
   a.err = c.d_err;
-  const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad;
+  const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad +
+                   p.s * b200::kTcThreads * (int)sizeof(u64);
   static int attr_set[64][2] = {};
   auto launch = [&](auto kernel, int which) {
     if (!attr_set[c.device][which]) {

@@ -181,8 +181,13 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 // built on the host per plan. Both use the canonical K-major layout without
 // swizzle: core matrices of 8 rows x 16 bytes stored as [k chunk][row group]
 // [8 rows][16 B], so SBO = 128 B and LBO = (rows / 8) * 128 B. Targets run in
-// groups of 8 through 64 TMEM columns; the MMA completion wait is bounded and
-// a timeout is reported through `err` (results of that CTA are then invalid).
+// groups of 8 through 64 TMEM columns. A CTA runs `tiles_per_cta` consecutive
+// 128-coefficient tiles; the next tile's s source rows are copied into shared
+// memory (cp.async) while the current tile's products and reductions run.
+// Every mbarrier wait is bounded: a timeout is reported through `err` (results
+// of that CTA are then invalid), and the CTA waits (bounded) for its own bulk
+// copy, matrix product and staged rows before it frees its TMEM and returns.
+// Dynamic shared memory: A (128 x kpad), B (groups x 64 x kpad), staging (s KiB).
 constexpr int kTcThreads = 128;
 constexpr int kTcGroupTargets = 8;
 constexpr int kTcGroupRows = 64;  // 8 targets x 8 output bytes
@@ -222,6 +227,21 @@ __host__ __device__ __forceinline__ int tc_canon(int r, int k, int rows) {
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+// Bounded wait for the completion of the mbarrier phase with the given parity.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+  uint32_t got = 0;
+  for (int it = 0; it < (1 << 20) && !got; ++it)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(got)
+        : "r"(bar), "r"(parity));
+  return got != 0;
+}
+// 16-byte global -> shared copy that completes asynchronously (cp.async.wait_group).
+__device__ __forceinline__ void tc_copy16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
 // Shared-memory matrix descriptor: SWIZZLE_NONE, Blackwell version 1.
 __device__ __forceinline__ u64 tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
   return u64((addr >> 4) & 0x3FFF) | (u64((lbo >> 4) & 0x3FFF) << 16) | (u64((sbo >> 4) & 0x3FFF) << 32) |
@@ -242,6 +262,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   uint8_t *sa = tc_smem;                      // 128 x kpad
   uint8_t *sb = tc_smem + kTcThreads * kpad;  // groups x 64 x kpad
   const uint32_t bbytes = uint32_t(a.groups * kTcGroupRows * kpad);
+  uint8_t *stage = sb + bbytes;                // s x 128 words: the next tile's source rows
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&bbar)), "r"(1));
@@ -276,33 +297,44 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   // idesc: S32 accumulate, unsigned 8-bit A and B, K-major, N = 64, M = 128.
   const uint32_t idesc = (2u << 4) | (uint32_t(kTcGroupRows >> 3) << 17) | (uint32_t(kTcThreads >> 4) << 24);
   const uint32_t tiles = uint32_t(n / kTcThreads);
-  bool ok = true;
+  // The s source rows of a tile (128 words each) are copied into `stage` while
+  // the previous tile's matrix products and reductions run.
+  auto stage_tile = [&](uint32_t tile) {
+    const u64 *rows = src + u64(tile) * kTcThreads;
+    for (int c = tid; c < s * (kTcThreads / 2); c += kTcThreads) {
+      const int j = c / (kTcThreads / 2), w = (c % (kTcThreads / 2)) * 2;
+      tc_copy16(stage + (j * kTcThreads + w) * sizeof(u64), rows + u64(j) * n + w);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const uint32_t first = blockIdx.x * uint32_t(a.tiles_per_cta);
+  if (first < tiles) stage_tile(first);
+  bool ok = true, b_pending = true, mma_pending = false;
   uint32_t phase = 0;  // completed MMA groups so far (mbarrier phase parity)
   for (int ti = 0; ti < a.tiles_per_cta && ok; ++ti) {
-    const uint32_t tile = blockIdx.x * a.tiles_per_cta + ti;
+    const uint32_t tile = first + ti;
     if (tile >= tiles) break;  // uniform across the CTA
     const u64 k = u64(tile) * kTcThreads + tid;
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const u64 *rows = reinterpret_cast<const u64 *>(stage);
     // A row of this thread's coefficient: the byte limbs of y_j, zero-padded.
     for (int j = 0; j < kpad / 8; ++j) {
-      const u64 y = j < s ? shoup_canon(src[u64(j) * n + k], sinv[j].w, sinv[j].wq, sq[j]) : 0;
+      const u64 y = j < s ? shoup_canon(rows[j * kTcThreads + tid], sinv[j].w, sinv[j].wq, sq[j]) : 0;
       *reinterpret_cast<u64 *>(sa + tc_canon(tid, j * 8, kTcThreads)) = y;  // little-endian bytes = limbs
     }
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
+    // Every thread has read the staged rows: bring in the next tile's.
+    if (ti + 1 < a.tiles_per_cta && tile + 1 < tiles) stage_tile(tile + 1);
     if (ti == 0) {  // B must have landed before the first MMA reads it
-      uint32_t got = 0;
-      for (int it = 0; it < (1 << 20) && !got; ++it)
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(got)
-            : "r"(smem_addr(&bbar)), "r"(0u));
-      if (!__syncthreads_and(got != 0)) {
+      if (!__syncthreads_and(tc_wait(smem_addr(&bbar), 0))) {
         ok = false;
         break;
       }
+      b_pending = false;
     }
     for (int g = 0; g < a.groups; ++g) {
       if (tid == 0) {
@@ -319,21 +351,15 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
             smem_addr(&mbar)));
       }
-      uint32_t done = 0;
-      for (int it = 0; it < (1 << 20) && !done; ++it)
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(smem_addr(&mbar)), "r"(phase & 1));
-      ++phase;
       // One decision for the whole CTA: every thread leaves together on a timeout.
-      const bool all_done = __syncthreads_and(done != 0);
+      const bool all_done = __syncthreads_and(tc_wait(smem_addr(&mbar), phase & 1));
       asm volatile("tcgen05.fence::after_thread_sync;");
       if (!all_done) {
         ok = false;
+        mma_pending = true;
         break;
       }
+      ++phase;
       const int tl_end = min(kTcGroupTargets, t_count - g * kTcGroupTargets);
       // Four targets' 8 columns per load, one wait per load.
       for (int tq = 0; tq < kTcGroupTargets; tq += 4) {
@@ -372,6 +398,11 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
     }
   }
   if (!ok && tid == 0) atomicExch(a.err, 1);
+  // Nothing may still write this CTA's shared memory or TMEM once it leaves:
+  // B, a timed-out matrix product and any staged rows are waited for (bounded).
+  if (b_pending) tc_wait(smem_addr(&bbar), 0);
+  if (mma_pending) tc_wait(smem_addr(&mbar), phase & 1);
+  asm volatile("cp.async.wait_all;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcGroupRows));
