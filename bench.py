@@ -243,7 +243,7 @@ def run_reference(args, rank, world):
 
 # ---- GPU side ------------------------------------------------------------------------------------
 # ---- configs 1-3: NTT and conversion legs -------------------------------------------------------
-def config_legs(nb, device, peak):
+def config_legs(nb, device, peak, peak_kind):
     """Config 1 (one 60-bit tower, forward + inverse), config 2 (8 x 32 towers, forward + inverse,
     direct launches and CUDA-graph replay) and config 3 (fused digits and ModDown at L = 24)."""
     import torch
@@ -265,7 +265,8 @@ def config_legs(nb, device, peak):
 
     def leg(ms, nbytes, **extra):
         gbs = nbytes / (ms / 1e3) / 1e9
-        return dict({"ms": ms, "algorithmic_bytes": nbytes, "gb_s": gbs, "frac_of_measured_hbm": gbs / peak}, **extra)
+        return dict({"ms": ms, "algorithmic_bytes": nbytes, "gb_s": gbs, "frac_of_hbm_peak": gbs / peak,
+                     "hbm_peak_source": peak_kind}, **extra)
 
     out = {}
     # config 1: the pinned OpenFHE 60-bit tower (q0, psi from the reference's pinned table).
@@ -639,7 +640,7 @@ def run_ours(args, rank, world, local):
 
     line["e2e"] = e2e
     line["plain"] = plain
-    line["configs"] = config_legs(nb, device, peaks()[0])
+    line["configs"] = config_legs(nb, device, *peaks())
     if not args.no_serving:
         line["serving"] = serving_legs(nb, device, value, plain["value"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
