@@ -248,7 +248,7 @@ def config_legs(nb, device, peak, peak_kind):
     direct launches and CUDA-graph replay) and config 3 (fused digits and ModDown at L = 24)."""
     import torch
 
-    from ntt_gpu_b200.params import find_primes, find_psi, synthetic_params, uniform_residues
+    from ntt_gpu_b200.params import find_primes, find_psi, min_psi, synthetic_params, uniform_residues
     W = 8 * N
 
     def timed(fn, iters):
@@ -279,33 +279,37 @@ def config_legs(nb, device, peak, peak_kind):
     c1.close()
     # config 2: 8 polynomials x 32 towers (16 x 50-bit and 16 x 60-bit, interleaved).
     q = [v for pair in zip(find_primes(N, 16, 50), find_primes(N, 16, 60)) for v in pair]
-    c2 = nb.Context(N, q, [find_psi(v, N) for v in q], device=device)
     x2 = nb.to_device(uniform_residues(N, q, SEED, polys=8), device)
     y2 = torch.empty_like(x2)
     ids = list(range(32))
-
-    def fwd_inv():
-        c2.ntt(y2, x2, ids, polys=8, poly_stride=32 * N)
-        c2.ntt(y2, y2, ids, polys=8, poly_stride=32 * N, inverse=True)
-
-    direct = timed(fwd_inv, 20)
-    graph = torch.cuda.CUDAGraph()
-    side = torch.cuda.Stream(device)
-    side.wait_stream(torch.cuda.current_stream(device))
-    with torch.cuda.stream(side):
-        fwd_inv()
-    torch.cuda.synchronize(device)
-    with torch.cuda.graph(graph):
-        fwd_inv()
-    replay = timed(graph.replay, 20)
-    exact = bool(torch.equal(y2, x2))
     nbytes = 8 * 32 * 2 * 2 * W
-    out["config2"] = {"workload": "N=2^16, 8 polynomials x 32 towers (16 x 50-bit + 16 x 60-bit), forward then "
-                                  "inverse; 512 MiB moved, larger than L2",
-                      "direct": leg(direct, nbytes), "graph_replay": leg(replay, nbytes),
-                      "roundtrip_exact": exact}
-    del graph
-    c2.close()
+
+    def config2_run(roots):
+        c2 = nb.Context(N, q, roots, device=device)
+
+        def fwd_inv():
+            c2.ntt(y2, x2, ids, polys=8, poly_stride=32 * N)
+            c2.ntt(y2, y2, ids, polys=8, poly_stride=32 * N, inverse=True)
+
+        direct = timed(fwd_inv, 20)
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device)
+        side.wait_stream(torch.cuda.current_stream(device))
+        with torch.cuda.stream(side):
+            fwd_inv()
+        torch.cuda.synchronize(device)
+        with torch.cuda.graph(graph):
+            fwd_inv()
+        replay = timed(graph.replay, 20)
+        exact = bool(torch.equal(y2, x2))
+        del graph
+        c2.close()
+        return {"direct": leg(direct, nbytes), "graph_replay": leg(replay, nbytes), "roundtrip_exact": exact}
+
+    out["config2"] = dict({"workload": "N=2^16, 8 polynomials x 32 towers (16 x 50-bit + 16 x 60-bit), forward "
+                                       "then inverse; 512 MiB moved, larger than L2"},
+                          **config2_run([find_psi(v, N) for v in q]))
+    out["config2"]["openfhe_min_roots"] = config2_run([min_psi(v, N) for v in q])
     # config 3: fused INTT -> ModUp -> NTT (Hybrid digits) and INTT -> ModDown -> NTT at L = 24.
     prm = synthetic_params(N, LEVEL, K_P, DNUM)
     c3 = nb.Context(prm.n, prm.q, prm.q_psi, prm.p, prm.p_psi, prm.alpha, device)
@@ -321,6 +325,44 @@ def config_legs(nb, device, peak, peak_kind):
     out["config3"] = {"workload": "N=2^16, L=24 (55-bit), K=8 (60-bit), dnum=3, one polynomial per call",
                       "mod_up_digits": leg(ms_d, W * (LEVEL + beta * T)),
                       "mod_down": leg(ms_m, W * (2 * LEVEL + K_P))}
+    # config 4: 16 ciphertexts at uneven levels L = {8, 16, 24}[i mod 3] in one request-table call, one
+    # shared key: key switch, relinearization (addends c0, c1) and rotation by one step (g = 5, with c0).
+    levels = [(8, 16, 24)[i % 3] for i in range(BATCH)]
+    c3.prepare(8)
+    c3.prepare(16)
+    qp = prm.q + prm.p
+    kb = device_residues(N, qp, SEED + 40, prm.full_digits(), device)
+    ka = device_residues(N, qp, SEED + 41, prm.full_digits(), device)
+    xs = device_residues(N, prm.q, SEED + 42, BATCH, device)
+    c0s = device_residues(N, prm.q, SEED + 43, BATCH, device)
+    outs = torch.empty((BATCH, 2, LEVEL, N), dtype=torch.int64, device=xs.device)
+
+    def requests(kind):
+        reqs = []
+        for i, lv in enumerate(levels):
+            ob, oa = outs[i, 0, :lv], outs[i, 1, :lv]
+            if kind == "rotate":
+                reqs.append(nb.make_request(lv, xs[i, :lv], ob, oa, kb, ka, c0=c0s[i, :lv], automorphism=5))
+            elif kind == "relinearize":
+                reqs.append(nb.make_request(lv, xs[i, :lv], ob, oa, kb, ka, add_b=ob, add_a=oa))
+            else:
+                reqs.append(nb.make_request(lv, xs[i, :lv], ob, oa, kb, ka))
+        return reqs
+
+    batch_bytes = W * (3 * sum(levels) + 2 * prm.digits(LEVEL) * (LEVEL + K_P))
+    c4 = {"workload": "N=2^16, K=8, dnum=3 (alpha=8), 16 ciphertexts at L = 8, 16, 24 (6 x 8, 5 x 16, 5 x 24) in "
+                      "one ntt_b200_keyswitch_requests call, one shared key; algorithmic bytes = input + 2 outputs "
+                      "per request + the key rows touched once",
+          "algorithmic_bytes": batch_bytes}
+    for kind in ("switch", "relinearize", "rotate"):
+        if kind == "relinearize":  # in place: the outputs start as (c0, c1) and receive the switch
+            outs[:, 0].copy_(c0s)
+            outs[:, 1].copy_(xs)
+        reqs = requests(kind)
+        ws = c3.requests_workspace(reqs)
+        ms = timed(lambda: c3.keyswitch_requests(reqs, ws), 20)
+        c4[kind] = dict(leg(ms, batch_bytes), keyswitch_per_s=BATCH / (ms / 1e3))
+    out["config4_uneven"] = c4
     c3.close()
     return out
 

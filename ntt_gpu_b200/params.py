@@ -65,6 +65,19 @@ def find_psi(q: int, n: int) -> int:
             return zeta
 
 
+def min_psi(q: int, n: int) -> int:
+    """The smallest primitive 2N-th root of unity mod q: the minimum over the N
+    odd powers of any one primitive root (OpenFHE's root convention, which the
+    reference pins in tests/openfhe_representation_tests.cpp:56-62)."""
+    psi = find_psi(q, n)
+    sq, power, best = psi * psi % q, psi, psi
+    for _ in range(n - 1):
+        power = power * sq % q
+        if power < best:
+            best = power
+    return best
+
+
 @dataclass
 class CkksParams:
     """N, M Q towers, K P towers, digit width alpha = ceil(M / dnum)."""
