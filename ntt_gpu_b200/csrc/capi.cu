@@ -420,6 +420,7 @@ Tunable g_tuning[] = {
     {"conv_tc", {1}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
     {"conv_tc_tiles", {4}, 1, 16},     // 128-coefficient tiles per tensor-core conversion CTA
+    {"conv_tc_fixed", {1}, 0, 1},      // tensor-core conversion kernels compiled for 8 -> 24/16/8 towers
 };
 Tunable *find_tunable(const char *name) {
   for (auto &t : g_tuning)
@@ -685,7 +686,7 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   a.err = c.d_err;
   const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad +
                    p.s * b200::kTcThreads * (int)sizeof(u64);
-  static int attr_set[64][2] = {};
+  static int attr_set[64][8] = {};
   auto launch = [&](auto kernel, int which) {
     if (!attr_set[c.device][which]) {
       CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
@@ -699,10 +700,20 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
     kernel<<<grid, b200::kTcThreads, smem, st>>>(a);
     t.done();
   };
-  if (lazy_out)
-    launch(b200::conv_tc_kernel<true>, 1);
-  else
-    launch(b200::conv_tc_kernel<false>, 0);
+  // The key switch's conversions (8 sources to 24, 16 or 8 targets: ModUp digits
+  // and ModDown with alpha = K = 8) run kernels compiled for their shape.
+  const int shape = tuned("conv_tc_fixed") && p.s == 8 ? (p.t == 24 ? 1 : p.t == 16 ? 2 : p.t == 8 ? 3 : 0) : 0;
+  const int which = 2 * shape + (lazy_out ? 1 : 0);
+  switch (which) {
+    case 0: launch(b200::conv_tc_kernel<false>, which); break;
+    case 1: launch(b200::conv_tc_kernel<true>, which); break;
+    case 2: launch(b200::conv_tc_kernel<false, 8, 24>, which); break;
+    case 3: launch(b200::conv_tc_kernel<true, 8, 24>, which); break;
+    case 4: launch(b200::conv_tc_kernel<false, 8, 16>, which); break;
+    case 5: launch(b200::conv_tc_kernel<true, 8, 16>, which); break;
+    case 6: launch(b200::conv_tc_kernel<false, 8, 8>, which); break;
+    default: launch(b200::conv_tc_kernel<true, 8, 8>, which); break;
+  }
 }
 
 // lazy_out: outputs in [0, 4m), only for a lazy forward NTT that consumes them.

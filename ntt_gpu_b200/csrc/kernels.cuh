@@ -248,7 +248,10 @@ __device__ __forceinline__ u64 tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo
          (u64(1) << 46);
 }
 
-template <bool LAZY_OUT>
+// FS, FT: when nonzero, the plan's source and target counts as compile-time
+// constants (the plan must have exactly FS sources and FT targets), so the
+// per-tile loops unroll; zero takes them from the plan at run time.
+template <bool LAZY_OUT, int FS = 0, int FT = 0>
 __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   extern __shared__ __align__(1024) uint8_t tc_smem[];
   __shared__ __align__(8) u64 mbar, bbar;
@@ -257,11 +260,13 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   __shared__ u64 sq[kMaxConvSources];
   __shared__ Shoup sinv[kMaxConvSources];
   const ConvPlan &p = *a.plan;
-  const int s = p.s, t_count = p.t, kpad = a.kpad;
+  const int s = FS ? FS : p.s, t_count = FT ? FT : p.t;
+  const int kpad = FS ? (8 * FS + 31) / 32 * 32 : a.kpad;
+  const int groups = FT ? (FT + kTcGroupTargets - 1) / kTcGroupTargets : a.groups;
   const int tid = threadIdx.x, warp = tid >> 5;
   uint8_t *sa = tc_smem;                      // 128 x kpad
   uint8_t *sb = tc_smem + kTcThreads * kpad;  // groups x 64 x kpad
-  const uint32_t bbytes = uint32_t(a.groups * kTcGroupRows * kpad);
+  const uint32_t bbytes = uint32_t(groups * kTcGroupRows * kpad);
   uint8_t *stage = sb + bbytes;                // s x 128 words: the next tile's source rows
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1));
@@ -319,6 +324,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
     __syncthreads();
     const u64 *rows = reinterpret_cast<const u64 *>(stage);
     // A row of this thread's coefficient: the byte limbs of y_j, zero-padded.
+#pragma unroll(FS ? 16 : 1)
     for (int j = 0; j < kpad / 8; ++j) {
       const u64 y = j < s ? shoup_canon(rows[j * kTcThreads + tid], sinv[j].w, sinv[j].wq, sq[j]) : 0;
       *reinterpret_cast<u64 *>(sa + tc_canon(tid, j * 8, kTcThreads)) = y;  // little-endian bytes = limbs
@@ -336,7 +342,8 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
       }
       b_pending = false;
     }
-    for (int g = 0; g < a.groups; ++g) {
+#pragma unroll(FT ? 10 : 1)
+    for (int g = 0; g < groups; ++g) {
       if (tid == 0) {
         for (int i = 0; i < kpad / 32; ++i) {
           const u64 da = tc_desc(smem_addr(sa) + i * 2 * (kTcThreads / 8) * 128, (kTcThreads / 8) * 128, 128);
@@ -362,6 +369,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
       ++phase;
       const int tl_end = min(kTcGroupTargets, t_count - g * kTcGroupTargets);
       // Four targets' 8 columns per load, one wait per load.
+#pragma unroll
       for (int tq = 0; tq < kTcGroupTargets; tq += 4) {
         if (tq >= tl_end) break;
         uint32_t v[32];
