@@ -45,8 +45,10 @@ __device__ __forceinline__ u64 sub_mod(u64 a, u64 b, u64 q) { return a >= b ? a 
 // xh*wh + hi(xl*wh) + hi(xh*wl): it drops xl*wl and every carry between the
 // partial products, so it is at most 2 below floor(x*w'/2^64), which is itself
 // at most 1 below floor(x*w/q). Hence x*w - estimate*q lies in [0, 4q); it is
-// formed mod 2^64 as x*w + estimate*(2^64 - q). Every product is a multiply-add,
-// none of them needs a carry fix-up, and no comparison is involved.
+// formed mod 2^64 as x*w + estimate*(2^64 - q). No product needs a carry
+// fix-up and no comparison is involved. The estimate's last term is a plain
+// 64-bit add, which leaves the multiply pipe (the NTT's bottleneck) to the
+// products.
 __device__ __forceinline__ u64 shoup_approx(u64 x, u64 w, u64 wq, u64 qneg) {
   const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32);
   const uint32_t wl = (uint32_t)wq, wh = (uint32_t)(wq >> 32);
@@ -55,7 +57,7 @@ __device__ __forceinline__ u64 shoup_approx(u64 x, u64 w, u64 wq, u64 qneg) {
   asm("mul.hi.u32 %0, %1, %2;" : "=r"(h1) : "r"(xl), "r"(wh));
   asm("mul.hi.u32 %0, %1, %2;" : "=r"(h2) : "r"(xh), "r"(wl));
   asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(qh) : "r"(xh), "r"(wh), "l"((u64)h1));
-  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(qh) : "r"(h2), "r"(1u), "l"(qh));
+  asm("add.u64 %0, %1, %2;" : "=l"(qh) : "l"(qh), "l"((u64)h2));
   asm("mul.lo.u64 %0, %1, %2;" : "=l"(r) : "l"(x), "l"(w));
   asm("mad.lo.u64 %0, %1, %2, %3;" : "=l"(r) : "l"(qh), "l"(qneg), "l"(r));
   return r;
