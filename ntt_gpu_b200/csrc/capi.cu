@@ -413,6 +413,7 @@ Tunable g_tuning[] = {
     {"ntt_minb_inv_col", {4}, 3, 4},
     {"ntt_col_direct", {1}, 0, 1},     // column passes load and store between registers and global memory
     {"ntt_row_direct", {1}, 0, 1},     // row passes load (forward) / store (inverse) mapping A directly
+    {"ntt_epi_stage", {0}, 0, 1},      // ModDown row pass stages its `left` rows in shared memory (measured slower)
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
@@ -465,6 +466,19 @@ void launch_row_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32
   const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
   const unsigned grid = persistent_grid(b200::ntt_row_ps<LOGN, MODE, INV>, smem, total, c.device, cache);
   b200::ntt_row_ps<LOGN, MODE, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
+}
+
+// The forward row pass of a ModDown launch with its `left` operand staged in
+// dynamic shared memory (the direct form).
+template <int LOGN, int MODE, int MINB>
+void launch_fwd_row_epi(const Ctx &c, const b200::NttBatch &b, dim3 grid, cudaStream_t st) {
+  static int attr_set[64] = {};
+  auto kernel = b200::ntt_fwd_row<LOGN, MODE, MINB, false, true, true>;
+  if (!attr_set[c.device]) {
+    CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, b200::kEpiSmemBytes));
+    attr_set[c.device] = 1;
+  }
+  kernel<<<grid, b200::kNttThreads, b200::kEpiSmemBytes, st>>>(b, c.tables);
 }
 
 template <int LOGN, int MODE>
@@ -521,7 +535,12 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     Timed t2("ntt_fwd_row", st);
     if (tuned("ntt_stage_tw_fwd_row"))
       NTT_LAUNCH(fwd_row, second, true, false);
-    else if (tuned("ntt_row_direct"))
+    else if (tuned("ntt_row_direct") && second.epi_left && tuned("ntt_epi_stage")) {
+      if (tuned("ntt_minb_fwd_row") == 3)
+        launch_fwd_row_epi<LOGN, MODE, 3>(c, second, grid, st);
+      else
+        launch_fwd_row_epi<LOGN, MODE, 4>(c, second, grid, st);
+    } else if (tuned("ntt_row_direct"))
       NTT_LAUNCH(fwd_row, second, false, true);
     else
       NTT_LAUNCH(fwd_row, second, false, false);

@@ -388,21 +388,41 @@ __device__ __forceinline__ Shoup staged_twiddle(const ulonglong2 *st, int k) {
 // row pass stores its outputs, straight between registers and global memory;
 // the other side stays staged through the warp's tile rows (mapping B puts the
 // lanes 128 bytes apart).
-template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT>
+// EPI_SMEM (ModDown launches of the direct form, b.epi_left set): each warp
+// copies its two rows of the epilogue's `left` operand into dynamic shared
+// memory (kEpiSmemBytes per CTA, rows of 256 words) with cp.async at kernel
+// start, so the epilogue reads them from shared memory after the butterflies.
+constexpr int kEpiSmemBytes = 16 * 256 * sizeof(u64);
+__device__ __forceinline__ void ntt_copy16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+
+template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT, bool EPI_SMEM = false>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
   static_assert(!(STW && DIRECT), "the staged-twiddle form has no direct variant");
+  static_assert(!EPI_SMEM || DIRECT, "the staged epilogue operand goes with the direct form");
   constexpr int LR = LOGN - 8;
   __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
+  extern __shared__ __align__(16) u64 epi_rows[];  // EPI_SMEM: 16 x 256 words of `left`
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
-  if (b.epi_left != nullptr && (threadIdx.x & 31) == 0) {
+  if (b.epi_left != nullptr) {
     // The ModDown epilogue reads its operands only after the butterflies:
-    // start moving this warp's two rows of them (4 KiB per operand) into L2 now.
+    // start moving this warp's two rows of them (4 KiB per operand) now.
     const u64 off = u64(b.off[blockIdx.z]) * (u64(1) << T.logn) + (row0 + 2 * (threadIdx.x >> 5)) * 256;
-    prefetch_l2(b.epi_left + blockIdx.y * b.epi_left_stride + off, 2 * 256 * sizeof(u64));
+    const u64 *lrows = b.epi_left + blockIdx.y * b.epi_left_stride + off;
+    if constexpr (EPI_SMEM) {
+      u64 *dst = epi_rows + 2 * (threadIdx.x >> 5) * 256;
+      for (int j = threadIdx.x & 31; j < 256; j += 32) ntt_copy16(dst + 2 * j, lrows + 2 * j);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    } else if ((threadIdx.x & 31) == 0) {
+      prefetch_l2(lrows, 2 * 256 * sizeof(u64));
+    }
     const u64 *add = poly_add(b, blockIdx.y);
-    if (add) prefetch_l2(add + off, 2 * 256 * sizeof(u64));
+    if (add && (threadIdx.x & 31) == 0) prefetch_l2(add + off, 2 * 256 * sizeof(u64));
   }
   const int r = threadIdx.x / 16, u = threadIdx.x % 16;
   const int row = row0 + r;
@@ -498,10 +518,15 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   const int j0 = STW ? int(threadIdx.x) : int(threadIdx.x & 31) + (int(threadIdx.x >> 5) * 2) * 128;
   const int j1 = STW ? 16 * 128 : j0 - int(threadIdx.x & 31) + 2 * 128;
   const int jstep = STW ? kNttThreads : 32;
+  if constexpr (EPI_SMEM) {  // this warp's own copies of its two rows
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncwarp();
+  }
   for (int j = j0; j < j1; j += jstep) {
     const int rr = j >> 7, c = (j & 127) * 2;
     const int sidx = rr * kRowPad + pad_col(c);
-    const ulonglong2 l = *reinterpret_cast<const ulonglong2 *>(left + rr * 256 + c);
+    const ulonglong2 l = EPI_SMEM ? *reinterpret_cast<const ulonglong2 *>(epi_rows + rr * 256 + c)
+                                  : *reinterpret_cast<const ulonglong2 *>(left + rr * 256 + c);
     ulonglong2 o;
     o.x = shoup_canon(sub_mod(l.x, tile[sidx], q), pinv.w, pinv.wq, q);
     o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
