@@ -98,6 +98,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("conv_limbs", (0, 1), ks_step, ("conv",), cuda_core_conv),
         ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",), cuda_core_conv),
         ("mac_limbs", (0, 1), ks_step, ("mac",), {}),
+        ("mac_approx", (0, 1), ks_step, ("mac",), {"mac_limbs": 0}),
         ("conv_tc", (0, 1), ks_step, ("conv",), {}),
         ("conv_tc_fixed", (0, 1), ks_step, ("conv",), {"conv_tc": 1}),
         ("conv_tc_tiles", (1, 2, 4, 8), ks_step, ("conv",), {"conv_tc": 1}),

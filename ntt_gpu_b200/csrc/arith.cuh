@@ -176,6 +176,27 @@ __device__ __forceinline__ u64 reduce128_lazy(u128 v, const Reducer &r) {
   const u64 hi = (u64)(v >> 64), lo = (u64)v;
   return shoup_lazy(hi, r.r64, r.r64q, r.m) + (lo - mulhi(lo, r.one) * r.m);
 }
+// x mod m in [0, 4m) for any x < 2^64 and m < 2^62: shoup_approx with w = 1
+// (one = floor(2^64 / m)), so x - e*m lies in [0, 4m) by the same argument.
+__device__ __forceinline__ u64 reduce64_approx(u64 x, u64 one, u64 mneg) {
+  const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32);
+  const uint32_t ol = (uint32_t)one, oh = (uint32_t)(one >> 32);
+  uint32_t h1, h2;
+  u64 e, r;
+  asm("mul.hi.u32 %0, %1, %2;" : "=r"(h1) : "r"(xl), "r"(oh));
+  asm("mul.hi.u32 %0, %1, %2;" : "=r"(h2) : "r"(xh), "r"(ol));
+  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(e) : "r"(xh), "r"(oh), "l"((u64)h1));
+  asm("add.u64 %0, %1, %2;" : "=l"(e) : "l"(e), "l"((u64)h2));
+  asm("mad.lo.u64 %0, %1, %2, %3;" : "=l"(r) : "l"(e), "l"(mneg), "l"(x));
+  return r;
+}
+// (hi * 2^64 + lo) mod m, canonical, for m < 2^61: each half reduced into
+// [0, 4m) with an approximate quotient, the sum (below 8m) brought to [0, m).
+__device__ __forceinline__ u64 reduce128_approx(u64 lo, u64 hi, const Reducer &r) {
+  const u64 mneg = 0 - r.m;
+  const u64 s = shoup_approx(hi, r.r64, r.r64q, mneg) + reduce64_approx(lo, r.one, mneg);
+  return csub_sign(csub_sign(csub_sign(s, 4 * r.m), 2 * r.m), r.m);
+}
 // (hi * 2^64 + lo) mod m, canonical, for any m < 2^63.
 __device__ __forceinline__ u64 reduce128(u64 lo, u64 hi, const Reducer &r) {
   const u64 a = csub(shoup_lazy(hi, r.r64, r.r64q, r.m), r.m);

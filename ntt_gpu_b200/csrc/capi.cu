@@ -417,6 +417,7 @@ Tunable g_tuning[] = {
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
+    {"mac_approx", {1}, 0, 1},         // MAC reductions with approximate quotients (moduli below 2^61)
     {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
     {"conv_tc", {1}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
@@ -924,6 +925,8 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
       constexpr int B = decltype(beta_tag)::value;
       if (wide)
         b200::mac2_kernel<B, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
+      else if (c.mode == 2 && tuned("mac_approx"))  // every modulus below 2^61
+        b200::mac2_kernel<B, false, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
       else
         b200::mac2_kernel<B, false><<<grid2, b200::kEwThreads, 0, st>>>(a);
     };

@@ -539,8 +539,11 @@ __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
 
 // Same MAC with a compile-time digit count and two adjacent coefficients per
 // thread (16-byte loads of every digit and key row).
-template <int BETA, bool WIDE>
+// APPROX (every modulus below 2^61, sums below 2^128): the final reductions
+// take approximate quotients (reduce128_approx); results are identical.
+template <int BETA, bool WIDE, bool APPROX = false>
 __global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
+  static_assert(!(WIDE && APPROX), "approximate reduction needs sums below 2^128");
   const u64 n = u64(1) << a.logn;
   const u64 i = (u64(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
   const int t = blockIdx.z;
@@ -569,10 +572,17 @@ __global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
   }
   const u64 o = z * a.poly_stride_out + t * n + i;
   ulonglong2 rb, ra;
-  rb.x = reduce(b0, red);
-  rb.y = reduce(b1, red);
-  ra.x = reduce(a0, red);
-  ra.y = reduce(a1, red);
+  if constexpr (APPROX) {
+    rb.x = reduce128_approx((u64)b0.v, (u64)(b0.v >> 64), red);
+    rb.y = reduce128_approx((u64)b1.v, (u64)(b1.v >> 64), red);
+    ra.x = reduce128_approx((u64)a0.v, (u64)(a0.v >> 64), red);
+    ra.y = reduce128_approx((u64)a1.v, (u64)(a1.v >> 64), red);
+  } else {
+    rb.x = reduce(b0, red);
+    rb.y = reduce(b1, red);
+    ra.x = reduce(a0, red);
+    ra.y = reduce(a1, red);
+  }
   if (a.accumulate) {
     const ulonglong2 ob = *reinterpret_cast<const ulonglong2 *>(a.out_b + o);
     const ulonglong2 oa = *reinterpret_cast<const ulonglong2 *>(a.out_a + o);
