@@ -174,7 +174,8 @@ struct ntt_b200_context_s {
   b200::DeviceTables tables{};
   size_t table_bytes = 0;
   std::mutex mu;
-  std::map<std::pair<std::vector<uint16_t>, std::vector<uint16_t>>, HostConvPlan> conv;
+  // (sources, targets, N^-1 folded into Bhat_j^-1) -> plan
+  std::map<std::tuple<std::vector<uint16_t>, std::vector<uint16_t>, bool>, HostConvPlan> conv;
   std::map<size_t, b200::DownPlan *> down;
   // Host-buffer pipeline (ntt_b200_keyswitch_host): two copy streams and the
   // per-slot events that hand the two device staging slots between them and
@@ -205,9 +206,13 @@ struct ntt_b200_context_s {
     cudaFree(d_inv);
   }
 
-  const HostConvPlan &conv_plan(const std::vector<uint16_t> &src, const std::vector<uint16_t> &tgt) {
+  // ninv: the plan expects its sources straight out of an unscaled inverse NTT
+  // (N times the coefficients, lazily reduced) and folds N^-1 into Bhat_j^-1,
+  // so y_j = [x_j * Bhat_j^-1 * N^-1]_{b_j} and every output is unchanged.
+  const HostConvPlan &conv_plan(const std::vector<uint16_t> &src, const std::vector<uint16_t> &tgt,
+                                bool ninv = false) {
     std::lock_guard<std::mutex> lock(mu);
-    auto key = std::make_pair(src, tgt);
+    auto key = std::make_tuple(src, tgt, ninv);
     auto it = conv.find(key);
     if (it != conv.end()) return it->second;
     require(!src.empty() && src.size() <= (size_t)b200::kMaxConvSources, "basis switch requires 1..40 source towers");
@@ -229,7 +234,8 @@ struct ntt_b200_context_s {
       for (int o = 0; o < s; ++o)
         if (o != j) hat = h_mul(hat, mod[src[o]] % b, b);
       plan->src_q[j] = b;
-      plan->src_inv[j] = h_shoup_pair(h_inv(hat, b), b);
+      const u64 hat_inv = h_inv(hat, b);
+      plan->src_inv[j] = h_shoup_pair(ninv ? h_mul(hat_inv, h_inv(n % b, b), b) : hat_inv, b);
       plan->src_id[j] = src[j];
       max_src = std::max(max_src, b);
       for (int i = 0; i < t; ++i) {
@@ -284,9 +290,10 @@ struct ntt_b200_context_s {
   }
 
   // Lookups that never build or upload a plan (nullptr when absent).
-  const HostConvPlan *find_conv_plan(const std::vector<uint16_t> &src, const std::vector<uint16_t> &tgt) {
+  const HostConvPlan *find_conv_plan(const std::vector<uint16_t> &src, const std::vector<uint16_t> &tgt,
+                                     bool ninv = false) {
     std::lock_guard<std::mutex> lock(mu);
-    auto it = conv.find(std::make_pair(src, tgt));
+    auto it = conv.find(std::make_tuple(src, tgt, ninv));
     return it == conv.end() ? nullptr : &it->second;
   }
   b200::DownPlan *find_down_plan(size_t level) {
@@ -413,6 +420,7 @@ Tunable g_tuning[] = {
     {"ntt_minb_inv_col", {4}, 3, 4},
     {"ntt_col_direct", {1}, 0, 1},     // column passes load and store between registers and global memory
     {"ntt_row_direct", {1}, 0, 1},     // row passes load (forward) / store (inverse) mapping A directly
+    {"intt_unscaled", {1}, 0, 1},      // inverse NTTs feeding a basis switch leave N^-1 to the switch
     {"ntt_epi_stage", {0}, 0, 1},      // ModDown row pass stages its `left` rows in shared memory (measured slower)
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
@@ -451,6 +459,9 @@ unsigned persistent_grid(Kernel kernel, int smem, uint32_t total, int device, in
   return (unsigned)std::min<uint64_t>(total, resident);
 }
 bool persistent_enabled() { return tuned("ntt_persistent") != 0; }
+// An inverse NTT that only feeds a basis switch skips N^-1 (folded into the
+// switch's plan) when the two-pass kernels run it.
+bool intt_unscaled(const Ctx &c) { return c.logn >= 12 && !persistent_enabled() && tuned("intt_unscaled") != 0; }
 
 template <int LOGN, int MODE, bool INV>
 void launch_col_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
@@ -501,6 +512,7 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     second.epi_pinv = fin->epi_pinv;
   }
   if (persistent_enabled()) {
+    require(!b.unscaled, "the persistent passes always scale by N^-1");
     const uint32_t ns = (uint32_t)slots, np = (uint32_t)polys;
     if (!inverse) {
       Timed t1("ntt_fwd_col", st);
@@ -556,10 +568,16 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
       NTT_LAUNCH(inv_row, b, false, false);
     t1.done();
     Timed t2("ntt_inv_col", st);
-    if (tuned("ntt_col_direct"))
+    if (second.unscaled) {
+      if (tuned("ntt_col_direct"))
+        NTT_LAUNCH(inv_col, second, true, true);
+      else
+        NTT_LAUNCH(inv_col, second, false, true);
+    } else if (tuned("ntt_col_direct")) {
       NTT_LAUNCH(inv_col, second, true);
-    else
+    } else {
       NTT_LAUNCH(inv_col, second, false);
+    }
     t2.done();
   }
 #undef NTT_LAUNCH
@@ -590,9 +608,10 @@ dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
 // src_list (device array, one entry per polynomial) replaces src / src_stride.
 void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots_in, size_t polys,
              u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr,
-             const u64 *const *src_list = nullptr) {
+             const u64 *const *src_list = nullptr, bool unscaled = false) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   require(!fin || !inverse, "final-pass redirection is forward only");
+  require(!unscaled || (inverse && c.logn >= 12), "unscaled transforms are two-pass inverses only");
   // Slots of one tower (e.g. the same target tower of several Hybrid digits)
   // run back to back, so its twiddle table is read from HBM once per launch.
   // Every slot carries its own offset and tower id, so the order changes no
@@ -611,6 +630,7 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
     b.src = src;
     b.dst = dst;
     b.src_list = src_list;
+    b.unscaled = unscaled;
     if (c.logn <= 11) {
       const dim3 grid(1, (unsigned)polys, (unsigned)count);
       const int threads = std::min<int>(b200::kNttThreads, std::max<int>(32, (int)(c.n / 2)));
@@ -817,9 +837,10 @@ void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst
   const size_t n = c.n, K = c.k;
   u64 *p_coeff = ws.take(polys * K * n);
   u64 *corr = ws.take(polys * L * n);
+  const bool unscaled = intt_unscaled(c);
   run_ntt(c, p_coeff, src + L * n, contiguous_slots(range_ids(c.m, c.m + K)), polys, src_stride, K * n,
-          true, st);
-  const auto &plan = c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L));
+          true, st, nullptr, nullptr, unscaled);
+  const auto &plan = c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L), unscaled);
   std::vector<uint16_t> slots;
   for (size_t i = 0; i < L; ++i) slots.push_back((uint16_t)i);
   run_conv(c, plan, corr, p_coeff, slots, polys, K * n, L * n, st, true);
@@ -846,7 +867,9 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
   const u64 dstride = beta * T * n;
   require(!(copy_own && src_list), "own-tower copies need a strided source");
   u64 *coeff = ws.take(polys * L * n);
-  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), polys, L * n, L * n, true, st, nullptr, src_list);
+  const bool unscaled = intt_unscaled(c);
+  run_ntt(c, coeff, src, contiguous_slots(range_ids(0, L)), polys, L * n, L * n, true, st, nullptr, src_list,
+          unscaled);
   const auto all = qp_ids(c, L);
   std::vector<Slot> fwd;
   size_t digit = 0;
@@ -864,7 +887,7 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
         slots.push_back((uint16_t)t);
         fwd.push_back({(uint32_t)(digit * T + t), all[t]});
       }
-    const auto &plan = c.conv_plan(range_ids(first, first + count), tgt);
+    const auto &plan = c.conv_plan(range_ids(first, first + count), tgt, unscaled);
     run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st, true);
   }
   run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st);
@@ -1348,7 +1371,9 @@ int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level) {
     Ctx &c = *ctx;
     const size_t L = level, K = c.k;
     c.conv_plan(range_ids(0, L), range_ids(c.m, c.m + K));
-    c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L));
+    // Both forms of the ModDown and digit plans: scaled (exact inverse NTT)
+    // and with N^-1 folded in (unscaled inverse NTT), whichever the tuning picks.
+    for (const bool ninv : {false, true}) c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L), ninv);
     c.down_plan(L);
     const auto all = qp_ids(c, L);
     for (size_t first = 0; first < L; first += c.alpha) {
@@ -1356,7 +1381,7 @@ int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level) {
       std::vector<uint16_t> tgt;
       for (size_t t = 0; t < L + K; ++t)
         if (t < first || t >= first + count) tgt.push_back(all[t]);
-      c.conv_plan(range_ids(first, first + count), tgt);
+      for (const bool ninv : {false, true}) c.conv_plan(range_ids(first, first + count), tgt, ninv);
     }
   });
 }
@@ -1600,7 +1625,7 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
     if (!workspace || workspace_bytes < need) throw WorkspaceError("workspace missing or too small");
     DeviceGuard guard(c.device);
     for (const Chunk &ch : chunks) {
-      c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, ch.level));
+      c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, ch.level), intt_unscaled(c));
       c.down_plan(ch.level);
     }
     const cudaStream_t st = as_stream(stream);
@@ -1645,7 +1670,7 @@ int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, si
     const size_t need = 2 * aligned_bytes(slot_words) + workspace_bytes(c, NTT_B200_OP_KEYSWITCH, level, chunk);
     if (!workspace || ws_size < need) throw WorkspaceError("workspace missing or too small");
     DeviceGuard guard(c.device);
-    c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level));
+    c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level), intt_unscaled(c));
     c.down_plan(level);
     std::lock_guard<std::mutex> lock(c.pipe_mu);
     if (!c.copy_in) {
@@ -1864,7 +1889,8 @@ int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, 
     if (need > kStaticScratchWords * sizeof(uint64_t))
       throw ContractError("ModDown scratch exceeds the 8 MiB static maximum of ntt_b200_mod_down_static "
                           "(needs (K + L) * N * 8 bytes); use ntt_b200_mod_down with a workspace");
-    require(c.find_conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level)) && c.find_down_plan(level),
+    require(c.find_conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level), intt_unscaled(c)) &&
+                c.find_down_plan(level),
             "ntt_b200_mod_down_static needs the level's tables: call ntt_b200_context_prepare(level) first");
     uint64_t *scratch = static_scratch(c.device);
     DeviceGuard guard(c.device);

@@ -58,6 +58,7 @@ struct NttBatch {
   const Shoup *epi_pinv;
   uint32_t off[kMaxSlots];
   uint16_t id[kMaxSlots];
+  bool unscaled;  // host side: inverse without N^-1 (selects the UNSCALED column pass)
 };
 
 __device__ __forceinline__ const u64 *poly_src(const NttBatch &b, u64 z) {
@@ -259,7 +260,11 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
   store_block<G::R, G::COLS, G::COLS, false>(tower_dst(b, T, fresh_block_ids()) + col0, tile, kStride);
 }
 
-template <int LOGN, int MODE, int MINB, bool DIRECT>
+// UNSCALED: the last stage is a plain Gentleman-Sande butterfly (no N^-1) and
+// the outputs stay lazily reduced: N times the coefficients, in [0, 4q) for
+// mode 2 and [0, 2q) for mode 1. For a basis switch that folds N^-1 into its
+// constants (conv_plan with ninv), which reduces its inputs itself.
+template <int LOGN, int MODE, int MINB, bool DIRECT, bool UNSCALED = false>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
@@ -316,9 +321,15 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
       gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
     }
   }
-  const Shoup ninv = v.c->ninv, last = v.c->last_inv;
+  if constexpr (UNSCALED) {
+    const ulonglong2 w = tw[1];  // stage 0: every pair (e, e + 8) uses T[1]
 #pragma unroll
-  for (int e = 0; e < 8; ++e) gs_last<MODE>(x[e], x[e + 8], ninv, last, q, q2);
+    for (int e = 0; e < 8; ++e) gs_butterfly<MODE>(x[e], x[e + 8], w.x, w.y, q, q2);
+  } else {
+    const Shoup ninv = v.c->ninv, last = v.c->last_inv;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) gs_last<MODE>(x[e], x[e + 8], ninv, last, q, q2);
+  }
   if constexpr (DIRECT) {
 #pragma unroll
     u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;

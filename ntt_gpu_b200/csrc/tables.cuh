@@ -40,8 +40,9 @@ constexpr int kLaneMajorMinLogn = 12;
 // Approximate-CRT switch from `s` source towers to `t` target towers
 // (include/ntt/basis_conversion.hpp:13-30):
 //   y_j = [x_j * Bhat_j^-1]_{b_j},  out_i = [sum_j y_j * [Bhat_j]_{m_i}]_{m_i}.
-// `scale` optionally folds a per-source constant into Bhat_j^-1 (e.g. N^-1
-// when the source arrives straight out of an unscaled inverse NTT).
+// Plans built with `ninv` fold N^-1 into Bhat_j^-1, for sources that arrive
+// straight out of an unscaled inverse NTT (N times the coefficients, lazily
+// reduced); y_j, and so every output, is the same as the scaled path's.
 constexpr int kMaxConvSources = 40;
 constexpr int kMaxConvTargets = 80;
 struct ConvPlan {
