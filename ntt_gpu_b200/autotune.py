@@ -94,6 +94,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("ntt_row_direct", (0, 1), ntt_step, ("ntt_fwd_row", "ntt_inv_row"), {}),
         ("ntt_epi_stage", (0, 1), ks_step, ("ntt_fwd_row",), {}),
         ("intt_unscaled", (0, 1), ks_step, ("ntt_inv_col",), {}),
+        ("digits_lazy", (0, 1), ks_step, ("ntt_fwd_row", "mac"), {}),
         ("ntt_stage_tw_fwd_row", (0, 1), ntt_step, ("ntt_fwd_row",), {}),
         ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",), {}),
         ("conv_limbs", (0, 1), ks_step, ("conv",), cuda_core_conv),

@@ -420,7 +420,8 @@ Tunable g_tuning[] = {
     {"ntt_minb_inv_col", {4}, 3, 4},
     {"ntt_col_direct", {1}, 0, 1},     // column passes load and store between registers and global memory
     {"ntt_row_direct", {1}, 0, 1},     // row passes load (forward) / store (inverse) mapping A directly
-    {"intt_unscaled", {1}, 0, 1},      // inverse NTTs feeding a basis switch leave N^-1 to the switch
+    {"intt_unscaled", {1}, 0, 1},
+    {"digits_lazy", {1}, 0, 1},        // Hybrid digits feeding the fused MAC skip their final reduction      // inverse NTTs feeding a basis switch leave N^-1 to the switch
     {"ntt_epi_stage", {0}, 0, 1},      // ModDown row pass stages its `left` rows in shared memory (measured slower)
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
@@ -462,6 +463,14 @@ bool persistent_enabled() { return tuned("ntt_persistent") != 0; }
 // An inverse NTT that only feeds a basis switch skips N^-1 (folded into the
 // switch's plan) when the two-pass kernels run it.
 bool intt_unscaled(const Ctx &c) { return c.logn >= 12 && !persistent_enabled() && tuned("intt_unscaled") != 0; }
+// Hybrid digits that only feed the fused MAC stay in the forward NTT's lazy
+// range [0, 8q): with every modulus below 2^61 and at most 4 digits, the MAC's
+// 128-bit sums stay below 2^127 and its reductions give canonical results. The
+// 30-bit-limb MAC needs inputs below 2^60, so it rules this out.
+bool digits_lazy(const Ctx &c, size_t beta) {
+  return c.mode == 2 && beta <= 4 && c.logn >= 12 && !persistent_enabled() && tuned("digits_lazy") != 0 &&
+         tuned("mac_limbs") == 0;
+}
 
 template <int LOGN, int MODE, bool INV>
 void launch_col_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
@@ -608,10 +617,11 @@ dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
 // src_list (device array, one entry per polynomial) replaces src / src_stride.
 void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots_in, size_t polys,
              u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr,
-             const u64 *const *src_list = nullptr, bool unscaled = false) {
+             const u64 *const *src_list = nullptr, bool unscaled = false, bool lazy_out = false) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   require(!fin || !inverse, "final-pass redirection is forward only");
   require(!unscaled || (inverse && c.logn >= 12), "unscaled transforms are two-pass inverses only");
+  require(!lazy_out || (!inverse && !fin && c.logn >= 12), "lazy outputs are two-pass forward transforms only");
   // Slots of one tower (e.g. the same target tower of several Hybrid digits)
   // run back to back, so its twiddle table is read from HBM once per launch.
   // Every slot carries its own offset and tower id, so the order changes no
@@ -631,6 +641,7 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
     b.dst = dst;
     b.src_list = src_list;
     b.unscaled = unscaled;
+    b.lazy_out = lazy_out;
     if (c.logn <= 11) {
       const dim3 grid(1, (unsigned)polys, (unsigned)count);
       const int threads = std::min<int>(b200::kNttThreads, std::max<int>(32, (int)(c.n / 2)));
@@ -861,7 +872,7 @@ void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst
 // (the fused MAC reads them from the input).
 // src_list (device array, one input per polynomial) replaces the strided src.
 void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carver &ws, bool copy_own,
-               cudaStream_t st, const u64 *const *src_list = nullptr) {
+               cudaStream_t st, const u64 *const *src_list = nullptr, bool lazy_out = false) {
   const size_t n = c.n, K = c.k, T = L + K;
   const size_t beta = 1 + (L - 1) / c.alpha;
   const u64 dstride = beta * T * n;
@@ -890,7 +901,7 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
     const auto &plan = c.conv_plan(range_ids(first, first + count), tgt, unscaled);
     run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st, true);
   }
-  run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st);
+  run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st, nullptr, nullptr, false, lazy_out);
 }
 
 // MAC of `polys` requests: out_b/out_a of request z at out + z * out_stride;
@@ -898,7 +909,7 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
 void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride,
             const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
             const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a, bool full_key_rows,
-            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr) {
+            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr, bool lazy_digits = false) {
   const size_t n = c.n, T = L + c.k;
   const size_t beta = digits.size();
   require(beta >= 1 && beta <= (size_t)b200::kMaxDigits &&
@@ -930,9 +941,11 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
   a.accumulate = accumulate;
   u64 max_q = 0;
   for (auto q : c.mod) max_q = std::max(max_q, q);
-  const u128 prod = (u128)(max_q - 1) * (max_q - 1);
+  // Lazy digits lie in [0, 8q).
+  const u128 prod = (u128)(lazy_digits ? 8 * max_q - 1 : max_q - 1) * (max_q - 1);
   const bool wide = prod > (~(u128)0) / (u128)beta;
   const bool limbs = max_q < (u64(1) << 60) && tuned("mac_limbs") != 0;
+  require(!lazy_digits || (!limbs && beta <= 4 && n >= 2 * b200::kEwThreads), "lazy digits need the 2-coefficient MAC");
   Timed t("mac", st);
   if (n >= 2 * b200::kEwThreads && beta <= 4 && limbs) {
     const dim3 grid2((unsigned)(n / (2 * b200::kEwThreads)), (unsigned)polys, (unsigned)T);
@@ -1009,11 +1022,12 @@ void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const 
   u64 *digits = ws.take(batch * beta * T * n);
   u64 *acc = ws.take(2 * batch * T * n);  // [batch][b|a][T][N]
   u64 *rot = ws.take(2 * batch * T * n);
-  do_digits(c, L, batch, digits, src, ws, false, st);
+  const bool lazy = digits_lazy(c, beta);
+  do_digits(c, L, batch, digits, src, ws, false, st, nullptr, lazy);
   std::vector<const u64 *> dptr;
   for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
   do_mac(c, L, batch, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, src, key_digits(c, key_b, beta),
-         key_digits(c, key_a, beta), true, false, st);
+         key_digits(c, key_a, beta), true, false, st, nullptr, lazy);
   const u64 *ext = acc;
   if (c0) {
     do_rotate(c, L, batch, rot, rot + T * n, acc, acc + T * n, 2 * T * n, c0, L * n, g, st);
@@ -1132,10 +1146,11 @@ void run_chunk(Ctx &c, const ntt_b200_ks_request *reqs, const Chunk &ch, Carver 
   u64 *digits = ws.take(u * beta * T * n);
   u64 *acc = ws.take(2 * r * T * n);  // [request][b|a][T][N]
   u64 *rot = ch.rotate ? ws.take(2 * r * T * n) : nullptr;
-  do_digits(c, L, u, digits, nullptr, ws, false, st, usrc);
+  const bool lazy = digits_lazy(c, beta);
+  do_digits(c, L, u, digits, nullptr, ws, false, st, usrc, lazy);
   std::vector<const u64 *> dptr;
   for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
-  do_mac(c, L, r, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, nullptr, {}, {}, true, false, st, desc);
+  do_mac(c, L, r, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, nullptr, {}, {}, true, false, st, desc, lazy);
   const u64 *ext = acc;
   if (ch.rotate) {
     do_rotate(c, L, r, rot, rot + T * n, acc, acc + T * n, 2 * T * n, nullptr, 0, 1, st, desc);

@@ -59,6 +59,7 @@ struct NttBatch {
   uint32_t off[kMaxSlots];
   uint16_t id[kMaxSlots];
   bool unscaled;  // host side: inverse without N^-1 (selects the UNSCALED column pass)
+  bool lazy_out;  // forward: leave the outputs in the butterflies' range ([0, 8q) in mode 2)
 };
 
 __device__ __forceinline__ const u64 *poly_src(const NttBatch &b, u64 z) {
@@ -500,9 +501,10 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
       }
     }
   }
+  const bool canonical = !b.lazy_out;
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
-    x[e] = reduce_final<MODE>(x[e], q, q2);
+    if (canonical) x[e] = reduce_final<MODE>(x[e], q, q2);
     my[pad_col(u * 16 + e)] = x[e];
   }
   if constexpr (STW) {
