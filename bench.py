@@ -679,6 +679,28 @@ def run_ours(args, rank, world, local):
            "h2d_bytes_per_step": int(h_x.numel() * 8), "d2h_bytes_per_step": int((h_b.numel() + h_a.numel()) * 8),
            "steps": e2e_steps, "api": f"ntt_b200_keyswitch_host, pinned host buffers, chunks of {chunk}",
            "outputs_equal_device_path": e2e_exact}
+    # The copy bound of that number: the same step's bytes moved by plain pinned copies alone, the outputs
+    # device-to-host while the inputs go host-to-device on another stream (no kernels).
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def copies_only():
+        with torch.cuda.stream(s_in):
+            d_x.copy_(h_x, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            h_b.copy_(out_b, non_blocking=True)
+            h_a.copy_(out_a, non_blocking=True)
+
+    for _ in range(2):
+        copies_only()
+    torch.cuda.synchronize(dev)
+    c0_ = time.perf_counter()
+    for _ in range(e2e_steps):
+        copies_only()
+    torch.cuda.synchronize(dev)
+    copy_s = (time.perf_counter() - c0_) / e2e_steps
+    e2e["copy_bound"] = {"value": B * world / copy_s, "unit": UNIT, "ms_per_step": copy_s * 1e3,
+                         "note": "pinned copies of the step's inputs and outputs only, both directions at once"}
+    e2e["frac_of_copy_bound"] = e2e["value"] / e2e["copy_bound"]["value"]
 
     line["e2e"] = e2e
     line["plain"] = plain

@@ -68,12 +68,13 @@ __device__ __forceinline__ u64 csub_sign(u64 x, u64 m) {
   return (int64_t)d < 0 ? x : d;
 }
 
-// Forward Cooley-Tukey (x, y) -> (x + w*y, x - w*y).
-template <int MODE>
+// Forward Cooley-Tukey (x, y) -> (x + w*y, x - w*y). FRESH (mode 2): x is a
+// transform input, already below 4q, so it needs no reduction first.
+template <int MODE, bool FRESH = false>
 __device__ __forceinline__ void ct_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 q, u64 q2) {
   if constexpr (MODE == 2) {
     const u64 q4 = 2 * q2;
-    const u64 a = csub_sign(x, q4);  // [0, 8q) -> [0, 4q)
+    const u64 a = FRESH ? x : csub_sign(x, q4);  // [0, 8q) -> [0, 4q)
     const u64 t = shoup_approx(y, w, wq, 0 - q);
     x = a + t;
     y = a + q4 - t;

@@ -214,7 +214,12 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
-      ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+      // Stage 0 reads the transform's inputs, below 4q (canonical, or a
+      // basis switch's lazy output), so mode 2 skips their first reduction.
+      if (s == 0)
+        ct_butterfly<MODE, true>(x[e], x[e + d], w.x, w.y, q, q2);
+      else
+        ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
     }
   }
   if constexpr (G::LR > 4) {
@@ -501,10 +506,14 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
       }
     }
   }
-  const bool canonical = !b.lazy_out;
+  // Mode 2 with the ModDown epilogue: the values only need to reach [0, 4q),
+  // since the epilogue forms (left + 4q - x) * P^-1 and reduces that itself.
+  const bool epi4 = MODE == 2 && b.epi_left != nullptr;
+  const bool canonical = !b.lazy_out && !epi4;
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
     if (canonical) x[e] = reduce_final<MODE>(x[e], q, q2);
+    else if (epi4) x[e] = csub_sign(x[e], 2 * q2);
     my[pad_col(u * 16 + e)] = x[e];
   }
   if constexpr (STW) {
@@ -541,8 +550,16 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
     const ulonglong2 l = EPI_SMEM ? *reinterpret_cast<const ulonglong2 *>(epi_rows + rr * 256 + c)
                                   : *reinterpret_cast<const ulonglong2 *>(left + rr * 256 + c);
     ulonglong2 o;
-    o.x = shoup_canon(sub_mod(l.x, tile[sidx], q), pinv.w, pinv.wq, q);
-    o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
+    if constexpr (MODE == 2) {
+      // left < q and x < 4q: left + 4q - x lies in (0, 5q), below 2^64 for q < 2^61;
+      // the approximate-quotient product lands in [0, 4q), two subtractions finish it.
+      const u64 q4 = 2 * q2, qneg = 0 - q;
+      o.x = csub_sign(csub_sign(shoup_approx(l.x + q4 - tile[sidx], pinv.w, pinv.wq, qneg), q2), q);
+      o.y = csub_sign(csub_sign(shoup_approx(l.y + q4 - tile[sidx + 1], pinv.w, pinv.wq, qneg), q2), q);
+    } else {
+      o.x = shoup_canon(sub_mod(l.x, tile[sidx], q), pinv.w, pinv.wq, q);
+      o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
+    }
     if (add) {
       const ulonglong2 e = *reinterpret_cast<const ulonglong2 *>(add + rr * 256 + c);
       o.x = add_mod(o.x, e.x, q);
