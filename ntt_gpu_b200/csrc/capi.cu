@@ -137,6 +137,26 @@ b200::Reducer h_reducer(u64 m) {
   return r;
 }
 
+// Dynamic shared memory limit of every tensor-core conversion kernel, raised
+// once per device when its first plan is built (so launches, also inside a
+// graph capture, make no attribute calls).
+void ensure_conv_tc_attributes(int device) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64 || done[device]) return;
+  const int bytes = 160 * 1024;
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<false, 8, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<true, 8, 24>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<false, 8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<true, 8, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<false, 8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CUDA_CHECK(cudaFuncSetAttribute(b200::conv_tc_kernel<true, 8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done[device] = true;
+}
+
 struct DeviceGuard {
   int previous = -1;
   explicit DeviceGuard(int device) {
@@ -285,6 +305,7 @@ struct ntt_b200_context_s {
       }
       CUDA_CHECK(cudaMalloc(&hp.tc_b, bm.size()));
       CUDA_CHECK(cudaMemcpy(hp.tc_b, bm.data(), bm.size(), cudaMemcpyHostToDevice));
+      ensure_conv_tc_attributes(device);
     }
     return conv.emplace(key, hp).first->second;
   }
@@ -737,12 +758,9 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   a.err = c.d_err;
   const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad +
                    p.s * b200::kTcThreads * (int)sizeof(u64);
-  static int attr_set[64][8] = {};
+  ensure_conv_tc_attributes(c.device);
   auto launch = [&](auto kernel, int which) {
-    if (!attr_set[c.device][which]) {
-      CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-      attr_set[c.device][which] = 1;
-    }
+    (void)which;
     const size_t tiles = c.n / b200::kTcThreads;
     const size_t per_cta = (size_t)tuned("conv_tc_tiles");
     a.tiles_per_cta = (int)per_cta;

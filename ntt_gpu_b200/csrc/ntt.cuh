@@ -241,7 +241,6 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
       }
     }
     if constexpr (DIRECT) {
-#pragma unroll
       u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;
 #pragma unroll
       for (int e = 0; e < 16; ++e) dst[G::row_b(e, u) * kStride] = x[e];
@@ -252,7 +251,6 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
     for (int e = 0; e < 16; ++e) tile[G::row_b(e, u) * G::COLS + c] = x[e];
   } else {
     if constexpr (DIRECT) {
-#pragma unroll
       u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;
 #pragma unroll
       for (int e = 0; e < 16; ++e) dst[G::row_a(e, u) * kStride] = x[e];
@@ -337,7 +335,6 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
     for (int e = 0; e < 8; ++e) gs_last<MODE>(x[e], x[e + 8], ninv, last, q, q2);
   }
   if constexpr (DIRECT) {
-#pragma unroll
     u64 *const dst = tower_dst(b, T, fresh_block_ids()) + col0 + c;
 #pragma unroll
     for (int e = 0; e < 16; ++e) dst[G::row_a(e, u) * kStride] = x[e];
@@ -640,16 +637,16 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
     u64 *const out = tower_dst(b, T, fresh_block_ids()) + row * 256 + u;
 #pragma unroll
     for (int e = 0; e < 16; ++e) out[e * 16] = x[e];
-    return;
-  }
-#pragma unroll
-  for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
-  if constexpr (STW) {
-    __syncthreads();
-    store_block<16, 256, kRowPad, true>(tower_dst(b, T, fresh_block_ids()) + row0 * 256, tile, 256);
   } else {
-    __syncwarp();
-    store_rows_warp(tower_dst(b, T, fresh_block_ids()) + row0 * 256, tile);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
+    if constexpr (STW) {
+      __syncthreads();
+      store_block<16, 256, kRowPad, true>(tower_dst(b, T, fresh_block_ids()) + row0 * 256, tile, 256);
+    } else {
+      __syncwarp();
+      store_rows_warp(tower_dst(b, T, fresh_block_ids()) + row0 * 256, tile);
+    }
   }
 }
 
