@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import shutil
 import subprocess
 from dataclasses import dataclass
 
@@ -31,13 +32,17 @@ def _ptr(a: np.ndarray | None):
 
 
 def build(force: bool = False) -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    """Compile liboracle.so (and oracle/_ref, CPU and CUDA, when the reference tree exists)."""
     target = os.path.join(HERE, "liboracle.so")
     if force or not os.path.exists(target):
         subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     ref = os.path.join(HERE, "_ref", "libntt_ref.so")
     if force or not os.path.exists(ref):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    # The reference's CUDA resident path (the second GPU comparator) needs nvcc.
+    ref_cuda = os.path.join(HERE, "_ref", "libntt_ref_cuda.so")
+    if (force or not os.path.exists(ref_cuda)) and shutil.which("nvcc"):
+        subprocess.run(["make", "-s", "-C", HERE, "refcuda"], check=True)
 
 
 class _Ctx(ctypes.Structure):
