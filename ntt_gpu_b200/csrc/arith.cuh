@@ -91,12 +91,13 @@ __device__ __forceinline__ void ct_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 
   }
 }
 
-// Inverse Gentleman-Sande (x, y) -> (x + y, (x - y) * w).
-template <int MODE>
+// Inverse Gentleman-Sande (x, y) -> (x + y, (x - y) * w). FRESH (mode 2): x and
+// y are canonical transform inputs, so x + y < 2q already lies in [0, 4q).
+template <int MODE, bool FRESH = false>
 __device__ __forceinline__ void gs_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 q, u64 q2) {
   if constexpr (MODE == 2) {
     const u64 q4 = 2 * q2;
-    const u64 s = csub_sign(x + y, q4);
+    const u64 s = FRESH ? x + y : csub_sign(x + y, q4);
     const u64 d = x + q4 - y;
     y = shoup_approx(d, w, wq, 0 - q);
     x = s;

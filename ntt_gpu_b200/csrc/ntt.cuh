@@ -612,7 +612,11 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
         const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
-        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+        // The first stage reads the inverse transform's canonical inputs.
+        if (sp == 7)
+          gs_butterfly<MODE, true>(x[e], x[e + d], w.w, w.wq, q, q2);
+        else
+          gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
   }
