@@ -605,6 +605,14 @@ def run_ours(args, rank, world, local):
                 (kernels["ntt_fwd_col"]["launches"] / args.steps),
                 "units": "2 x 524288 B (read + write) per tower-transform; "
                          f"{fwd_towers_per_step} forward tower-transforms per step"}
+        # The ceiling that binds the passes: the integer multiply pipe, calibrated on this GPU by
+        # register-only mode-2 butterflies (the NTT's own arithmetic, no memory traffic).
+        rate = nb.butterfly_rate(device)
+        fwd_butterflies = fwd_towers_per_step * (N // 2) * (N.bit_length() - 1)
+        roof["compute"] = {"bound": "integer multiply pipe (mode-2 butterflies)",
+                           "achieved": fwd_butterflies / (fwd_ms / 1000.0), "peak": rate, "unit": "butterflies/s",
+                           "frac": fwd_butterflies / (fwd_ms / 1000.0) / rate,
+                           "peak_source": "ntt_b200_butterfly_rate: register-only mode-2 butterflies, this GPU"}
     total_kernel_ms = sum(k["total_ms"] for k in kernels.values()) or 1.0
     for k in kernels.values():
         k["share"] = k["total_ms"] / total_kernel_ms

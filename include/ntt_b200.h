@@ -385,6 +385,14 @@ int ntt_b200_timing_enable(int on);
 int ntt_b200_timing_reset(void);
 int ntt_b200_timing_query(const char *kernel, uint64_t *launches, double *total_ms);
 
+/* Calibration, with no counterpart in the reference: the running device's
+ * rate of the forward NTT's mode-2 butterflies (moduli below 2^61) with every
+ * operand in registers and no memory traffic, i.e. the integer-multiply
+ * ceiling the NTT passes are measured against. Runs about 10 ms of work on a
+ * private stream of `device`, allocates 8 bytes of device memory for the
+ * duration, and waits for the result. */
+int ntt_b200_butterfly_rate(int device, double *butterflies_per_second);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,7 @@ _SIGNATURES = {
     "ntt_b200_timing_enable": ([_I], _I),
     "ntt_b200_timing_reset": ([], _I),
     "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),
+    "ntt_b200_butterfly_rate": ([_I, ctypes.POINTER(ctypes.c_double)], _I),
 }
 
 
@@ -493,6 +494,14 @@ class KeyCache:
 
 KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col", "ntt_small", "conv", "mac",
                   "rotate", "correct", "pointwise", "table")
+
+
+def butterfly_rate(device: int = 0) -> float:
+    """Mode-2 NTT butterflies per second on `device` with operands in registers
+    (ntt_b200_butterfly_rate): the multiply-pipe ceiling of the NTT passes."""
+    out = ctypes.c_double()
+    _check(load().ntt_b200_butterfly_rate(int(device), ctypes.byref(out)))
+    return out.value
 
 
 def timing_enable(on: bool = True):

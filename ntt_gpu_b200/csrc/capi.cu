@@ -1233,6 +1233,51 @@ extern "C" {
 const char *ntt_b200_last_error(void) { return g_last_error.c_str(); }
 uint64_t ntt_b200_kernel_launches(void) { return g_launches.load(); }
 
+int ntt_b200_butterfly_rate(int device, double *butterflies_per_second) {
+  return guarded([&] {
+    require(butterflies_per_second != nullptr, "null output");
+    DeviceGuard guard(device);
+    const u64 q = 1152921504606584833ull;  // a 60-bit NTT prime (mode-2 range)
+    const b200::Shoup w[4] = {h_shoup_pair(18043022392882ull % q, q), h_shoup_pair(123456789012345ull, q),
+                              h_shoup_pair(q / 3, q), h_shoup_pair(q - 5, q)};
+    const unsigned grid = (unsigned)(4 * device_sms(device));
+    u64 *sink = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_CHECK(cudaMalloc(&sink, sizeof(u64)));
+    auto cleanup = [&] {
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      if (st) cudaStreamDestroy(st);
+      cudaFree(sink);
+    };
+    try {
+      CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      CUDA_CHECK(cudaEventCreate(&e0));
+      CUDA_CHECK(cudaEventCreate(&e1));
+      auto timed_run = [&](int rounds) {
+        CUDA_CHECK(cudaEventRecord(e0, st));
+        b200::butterfly_rate_kernel<<<grid, b200::kNttThreads, 0, st>>>(sink, q, w[0], w[1], w[2], w[3], rounds);
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaEventRecord(e1, st));
+        CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        return (double)ms;
+      };
+      timed_run(16);  // warm-up
+      const double probe = timed_run(64);
+      const int rounds = (int)std::max(64.0, std::min(1e6, 64.0 * 10.0 / std::max(probe, 1e-3)));
+      const double ms = timed_run(rounds);
+      *butterflies_per_second = double(grid) * b200::kNttThreads * rounds * 32.0 / (ms * 1e-3);
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
+  });
+}
+
 int ntt_b200_tuning_set(const char *name, int64_t value) {
   return guarded([&] {
     Tunable *t = find_tunable(name);

@@ -697,4 +697,35 @@ __global__ void __launch_bounds__(kNttThreads) ntt_small(NttBatch b, DeviceTable
   for (int i = threadIdx.x; i < n; i += blockDim.x) v.dst[i] = a[i];
 }
 
+// ---- butterfly-rate calibration ------------------------------------------------
+// The forward NTT's arithmetic alone: each thread keeps 16 values in registers
+// and runs `rounds` radix-16 rounds (4 stages x 8 mode-2 Cooley-Tukey
+// butterflies) with twiddles held in registers, with no memory traffic. The
+// values stay in [0, 8q); they are folded into one word that is stored only
+// if it equals a fixed constant, so the work cannot be dropped. This measures
+// the multiply-pipe ceiling that bounds the NTT passes on the running GPU.
+__global__ void __launch_bounds__(kNttThreads, 4)
+    butterfly_rate_kernel(u64 *sink, u64 q, Shoup w0, Shoup w1, Shoup w2, Shoup w3, int rounds) {
+  const u64 q2 = 2 * q;
+  u64 x[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = (u64(blockIdx.x) * 4096 + threadIdx.x * 16 + e) % q;
+  for (int r = 0; r < rounds; ++r) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int d = 8 >> s;
+      const Shoup w = s == 0 ? w0 : s == 1 ? w1 : s == 2 ? w2 : w3;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        ct_butterfly<2>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
+    }
+  }
+  u64 fold = 0;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) fold ^= x[e];
+  if (fold == 0x9E3779B97F4A7C15ull) sink[0] = fold;
+}
+
 }  // namespace b200
