@@ -759,8 +759,7 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad +
                    p.s * b200::kTcThreads * (int)sizeof(u64);
   ensure_conv_tc_attributes(c.device);
-  auto launch = [&](auto kernel, int which) {
-    (void)which;
+  auto launch = [&](auto kernel) {
     const size_t tiles = c.n / b200::kTcThreads;
     const size_t per_cta = (size_t)tuned("conv_tc_tiles");
     a.tiles_per_cta = (int)per_cta;
@@ -772,16 +771,15 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   // The key switch's conversions (8 sources to 24, 16 or 8 targets: ModUp digits
   // and ModDown with alpha = K = 8) run kernels compiled for their shape.
   const int shape = tuned("conv_tc_fixed") && p.s == 8 ? (p.t == 24 ? 1 : p.t == 16 ? 2 : p.t == 8 ? 3 : 0) : 0;
-  const int which = 2 * shape + (lazy_out ? 1 : 0);
-  switch (which) {
-    case 0: launch(b200::conv_tc_kernel<false>, which); break;
-    case 1: launch(b200::conv_tc_kernel<true>, which); break;
-    case 2: launch(b200::conv_tc_kernel<false, 8, 24>, which); break;
-    case 3: launch(b200::conv_tc_kernel<true, 8, 24>, which); break;
-    case 4: launch(b200::conv_tc_kernel<false, 8, 16>, which); break;
-    case 5: launch(b200::conv_tc_kernel<true, 8, 16>, which); break;
-    case 6: launch(b200::conv_tc_kernel<false, 8, 8>, which); break;
-    default: launch(b200::conv_tc_kernel<true, 8, 8>, which); break;
+  switch (2 * shape + (lazy_out ? 1 : 0)) {
+    case 0: launch(b200::conv_tc_kernel<false>); break;
+    case 1: launch(b200::conv_tc_kernel<true>); break;
+    case 2: launch(b200::conv_tc_kernel<false, 8, 24>); break;
+    case 3: launch(b200::conv_tc_kernel<true, 8, 24>); break;
+    case 4: launch(b200::conv_tc_kernel<false, 8, 16>); break;
+    case 5: launch(b200::conv_tc_kernel<true, 8, 16>); break;
+    case 6: launch(b200::conv_tc_kernel<false, 8, 8>); break;
+    default: launch(b200::conv_tc_kernel<true, 8, 8>); break;
   }
 }
 

@@ -534,14 +534,18 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   if (add) add += rows_off;
   // Epilogue over the rows this thread's group owns: every row with STW (the
   // CTA synchronised above), the warp's own two rows otherwise.
+  // Either way each thread handles 8 chunks of 2 words; the fixed trip count
+  // lets every chunk's loads be in flight together.
   const int j0 = STW ? int(threadIdx.x) : int(threadIdx.x & 31) + (int(threadIdx.x >> 5) * 2) * 128;
-  const int j1 = STW ? 16 * 128 : j0 - int(threadIdx.x & 31) + 2 * 128;
-  const int jstep = STW ? kNttThreads : 32;
+  constexpr int kJStep = STW ? kNttThreads : 32;
+  static_assert(8 * kJStep * (STW ? 1 : 8) == 16 * 128, "8 chunks per thread cover the CTA's 16 rows");
   if constexpr (EPI_SMEM) {  // this warp's own copies of its two rows
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncwarp();
   }
-  for (int j = j0; j < j1; j += jstep) {
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int j = j0 + it * kJStep;
     const int rr = j >> 7, c = (j & 127) * 2;
     const int sidx = rr * kRowPad + pad_col(c);
     const ulonglong2 l = EPI_SMEM ? *reinterpret_cast<const ulonglong2 *>(epi_rows + rr * 256 + c)
