@@ -761,7 +761,11 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   ensure_conv_tc_attributes(c.device);
   auto launch = [&](auto kernel) {
     const size_t tiles = c.n / b200::kTcThreads;
-    const size_t per_cta = (size_t)tuned("conv_tc_tiles");
+    // The tuned tiles per CTA, halved while the grid would cover fewer than 4
+    // CTAs per SM (small batches: one request's switch is only 512 tiles).
+    size_t per_cta = (size_t)tuned("conv_tc_tiles");
+    const size_t want = 4 * (size_t)device_sms(c.device);
+    while (per_cta > 1 && ((tiles + per_cta - 1) / per_cta) * polys < want) per_cta = (per_cta + 1) / 2;
     a.tiles_per_cta = (int)per_cta;
     const dim3 grid((unsigned)((tiles + per_cta - 1) / per_cta), 1, (unsigned)polys);
     Timed t("conv", st);
