@@ -321,6 +321,21 @@ class Context:
         _check(self._lib.ntt_b200_hybrid_mac(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(digits),
                                              _ptr(key_b), _ptr(key_a), _stream(stream)))
 
+    def hybrid_mac_digits(self, level, out_b, out_a, digits, keys_b, keys_a, full_key_rows=True,
+                          accumulate=False, stream=None):
+        """MAC over per-digit buffers (lists of device tensors, one entry per digit).
+
+        full_key_rows: keys are full-context digits (M+K towers) rather than packed
+        active QP rows. accumulate: add into out_b/out_a instead of overwriting."""
+        count = len(digits)
+        if not (len(keys_b) == len(keys_a) == count):
+            raise ContractError("one key_b and one key_a buffer per digit")
+        vec = ctypes.c_void_p * max(1, count)
+        _check(self._lib.ntt_b200_hybrid_mac_digits(
+            self._h, level, _ptr(out_b), _ptr(out_a), vec(*[_ptr(d) for d in digits]),
+            vec(*[_ptr(k) for k in keys_b]), vec(*[_ptr(k) for k in keys_a]), count, int(full_key_rows),
+            int(accumulate), _stream(stream)))
+
     def hybrid_rotate(self, level, out_b, out_a, ext_b, ext_a, c0, automorphism, stream=None):
         _check(self._lib.ntt_b200_hybrid_rotate(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(ext_b),
                                                 _ptr(ext_a), _ptr(c0), automorphism, _stream(stream)))
