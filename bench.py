@@ -443,8 +443,12 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
 
     from ntt_gpu_b200.params import synthetic_params
     budget = 40 << 30
-    served_cfg = {"lanes": 2, "max_batch": BATCH, "depth": 1, "hbm_budget_bytes": budget}
-    plain_cfg = {"lanes": 1, "max_batch": 1, "depth": 2, "hbm_budget_bytes": budget}
+    # Served: 4 lanes, 2 waves deep, and a new wave only while the waves in flight hold
+    # less than 512 MiB of workspace (about four requests at the headline shape), so
+    # small mixed requests run many at a time and large ones gather into full waves.
+    served_cfg = {"lanes": 4, "max_batch": BATCH, "depth": 2, "hbm_budget_bytes": budget,
+                  "max_inflight_bytes": 512 << 20}
+    plain_cfg = {"lanes": 1, "max_batch": 1, "depth": 2, "hbm_budget_bytes": budget, "max_inflight_bytes": 0}
     legs = (("served", served_cfg), ("plain", plain_cfg))
     out = {"served_server": served_cfg,
            "plain_server": dict(plain_cfg, note="same kernels, one request per wave, the next request queued "
@@ -455,10 +459,15 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
     w = Workload(nb, prm, device, seed)
     head = []
     rates = sorted({round(plain_value * f) for f in (0.5, 0.9, 1.3)} | {round(batched_value * 0.9)})
+    # Each lane's arena is sized up front for the largest wave it can carry, so no
+    # arena grows (and waits on the driver for memory) while requests are timed.
+    wave_bytes = {b: w.ctx.requests_workspace_bytes([w.request(nb, LEVEL, "switch", 0, i) for i in range(b)])
+                  for b in (1, BATCH)}
     for rate in rates:
         row = {}
         for name, cfg in legs:
             srv = nb.Server(device=device, **cfg)
+            srv.reserve(wave_bytes[cfg["max_batch"]])
             count = max(64, min(400, int(rate * 0.12)))
             jobs = [(w.ctx, w.request(nb, LEVEL, "switch", 0, i)) for i in range(count)]
             # Warm-up: a burst sizes every lane's workspace arena for full waves.
@@ -492,7 +501,10 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
             jobs.append((wk.ctx, wk.request(nb, level, kind, step, i)))
         return jobs
 
+    mixed_bytes = {b: max(wk.ctx.requests_workspace_bytes([wk.request(nb, 32, "rotate", 1, i) for i in range(b)])
+                          for wk in works.values()) for b in (1, BATCH)}
     srv = nb.Server(device=device, **served_cfg)
+    srv.reserve(mixed_bytes[served_cfg["max_batch"]])
     burst = mixed_jobs(600, seed + 3)
     serve_poisson(nb, srv, burst[:40], 1e6, seed + 4)
     cap = serve_poisson(nb, srv, burst, 1e7, seed + 5)["throughput"]  # saturation: all arrive at once
@@ -503,6 +515,7 @@ def serving_legs(nb, device, batched_value, plain_value, seed=0x5E7E):
         row = {}
         for name, cfg in legs:
             srv = nb.Server(device=device, **cfg)
+            srv.reserve(mixed_bytes[cfg["max_batch"]])
             jobs = mixed_jobs(max(100, min(600, int(rate * 0.25))), seed + 7)
             serve_poisson(nb, srv, burst[:2 * BATCH * cfg["lanes"]], 1e7, seed + 6)  # warm-up burst
             row[name] = serve_poisson(nb, srv, jobs, rate, seed + 8)

@@ -241,7 +241,8 @@ int ntt_b200_keycache_trim(ntt_b200_keycache cache, size_t *freed);
  * device-resident ciphertexts and keys that the caller keeps alive until the
  * ticket completes. A scheduler thread forms waves of the oldest pending
  * request's (context, level) class, up to max_batch, and launches each on the
- * least-loaded lane (a CUDA stream with fewer than `depth` waves in flight)
+ * least-loaded lane (a CUDA stream with fewer than `depth` waves in flight),
+ * while the waves in flight hold less than max_inflight_bytes of workspace,
  * once its workspace fits the lane's arena, grown within hbm_budget_bytes
  * (the sum of all lanes' arenas; idle lanes give theirs back when needed): requests arriving while others run join the next
  * wave as lanes and memory free up, and waves on different lanes overlap on
@@ -255,6 +256,11 @@ typedef struct ntt_b200_server_config {
   int max_batch;  /* requests per wave, 1..1024 */
   int depth;      /* waves in flight per lane, 1..8 (0 = 1); >1 queues the next wave behind the running one */
   size_t hbm_budget_bytes; /* sum of the lanes' workspace arenas */
+  /* 0 = no limit. Otherwise a new wave launches only while the waves in flight
+   * hold less than this much workspace: small waves (low levels, small N) then
+   * run many at a time, up to lanes x depth, while large ones run a few at a
+   * time and the requests behind them gather into fuller waves. */
+  size_t max_inflight_bytes;
 } ntt_b200_server_config;
 typedef struct ntt_b200_ticket_info {
   int status;          /* NTT_B200_OK or the request's error */
@@ -286,6 +292,12 @@ int ntt_b200_server_drain(ntt_b200_server srv, uint32_t timeout_ms);
 int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int reset);
 /* Finishes pending and in-flight work, then frees the server. */
 int ntt_b200_server_destroy(ntt_b200_server srv);
+/* Grows every lane's workspace arena that has no wave in flight to at least
+ * bytes_per_lane, in stream order on the lane's stream, so that waves up to that
+ * size never wait for an arena to grow. A contract error if the arenas would
+ * exceed hbm_budget_bytes. (No counterpart in the reference, which has no
+ * server; its Limits reserve memory per Session, src/resident.cpp:10-28.) */
+int ntt_b200_server_reserve(ntt_b200_server srv, size_t bytes_per_lane);
 /* Requests submitted with key_b == key_a == NULL take their key from `cache`
  * by key_id: each wave acquires its keys on its lane's stream at launch and
  * releases them in stream order after it. A wave whose keys do not fit the

@@ -6,8 +6,9 @@
 //  - a wave is the oldest pending request's shape class (context, level) plus
 //    every later pending request of that class, up to max_batch;
 //  - a wave launches as soon as a lane (a CUDA stream) has fewer than `depth`
-//    waves in flight and its workspace fits the HBM budget next to the waves
-//    already in flight, so requests that arrive while others run are admitted
+//    waves in flight, the waves in flight hold less workspace than
+//    max_inflight_bytes (the measure of how much of the GPU they occupy), and
+//    its workspace fits the HBM budget next to the waves already in flight, so requests that arrive while others run are admitted
 //    as lanes and memory free up, and waves on different lanes overlap on the
 //    device (a depth above 1 queues the next wave behind the running one);
 //  - each lane owns a workspace arena that its waves reuse in stream order; an
@@ -90,6 +91,7 @@ struct ntt_b200_server_s {
   int depth = 1;
   uint64_t next_id = 1;
   size_t in_use = 0, peak_in_use = 0;
+  size_t work_in_flight = 0;  // workspace bytes of the waves in flight
   bool stopping = false;
   std::string fatal;  // first CUDA failure; the server refuses new work after it
   std::thread sched;
@@ -136,6 +138,7 @@ struct ntt_b200_server_s {
       }
       if (!ok && fatal.empty()) fatal = why;
       lanes[w.lane].inflight -= 1;
+      work_in_flight -= w.bytes;
       event_pool.push_back(w.done);
       it = waves_in_flight.erase(it);
       cv_done.notify_all();
@@ -170,10 +173,20 @@ struct ntt_b200_server_s {
       pending.clear();
       return false;
     }
-    int lane = -1;  // the lane with the fewest waves in flight, below the depth
-    for (size_t i = 0; i < lanes.size(); ++i)
-      if (lanes[i].inflight < depth && (lane < 0 || lanes[i].inflight < lanes[lane].inflight)) lane = (int)i;
+    // The lane with the fewest waves in flight, below the depth; among those,
+    // the one with the largest arena, so grown arenas are reused rather than
+    // new ones grown (an arena's growth can wait on the driver for memory).
+    int lane = -1;
+    for (size_t i = 0; i < lanes.size(); ++i) {
+      if (lanes[i].inflight >= depth) continue;
+      if (lane < 0 || lanes[i].inflight < lanes[lane].inflight ||
+          (lanes[i].inflight == lanes[lane].inflight && lanes[i].arena_bytes > lanes[lane].arena_bytes))
+        lane = (int)i;
+    }
     if (lane < 0) return false;
+    // Enough work in flight to occupy the GPU: let the pending requests gather
+    // into a fuller wave. Nothing in flight means no limit, so this never stalls.
+    if (cfg.max_inflight_bytes && work_in_flight >= cfg.max_inflight_bytes) return false;
     const Ticket &head = tickets[pending.front()];
     const ntt_b200_context ctx = head.ctx;
     const uint32_t level = head.req.level;
@@ -271,7 +284,7 @@ struct ntt_b200_server_s {
     auto owned = std::make_unique<Wave>();
     owned->lane = lane;
     owned->ids = wave;
-    owned->bytes = need;  // informational: the lane's arena holds the memory
+    owned->bytes = need;  // the lane's arena holds the memory; counted as work in flight
     owned->done = take_event();
     cudaEvent_t done = owned->done;
     lanes[lane].inflight += 1;
@@ -327,6 +340,7 @@ struct ntt_b200_server_s {
       if (rc == NTT_B200_ERR_CUDA && fatal.empty()) fatal = why;
       return true;
     }
+    work_in_flight += owned->bytes;
     waves_in_flight.push_back(std::move(owned));
     waves += 1;
     wave_requests += wave.size();
@@ -534,6 +548,36 @@ int ntt_b200_server_stats(ntt_b200_server srv, ntt_b200_server_report *out, int 
       srv->first_submit = srv->last_done = srv->queue_us = 0;
       srv->peak_in_use = srv->in_use;
     }
+    return NTT_B200_OK;
+  });
+}
+
+int ntt_b200_server_reserve(ntt_b200_server srv, size_t bytes_per_lane) {
+  return server_guard([&] {
+    if (!srv) return contract("null server");
+    std::lock_guard<std::mutex> lock(srv->mu);
+    // Lanes with waves in flight (or a launch being enqueued, which counts as in
+    // flight) keep their arenas; the others grow to bytes_per_lane.
+    size_t after = srv->in_use;
+    for (const Lane &ln : srv->lanes)
+      if (ln.inflight == 0 && ln.arena_bytes < bytes_per_lane) after += bytes_per_lane - ln.arena_bytes;
+    if (after > srv->cfg.hbm_budget_bytes) return contract("reservation exceeds the server's HBM budget");
+    for (Lane &ln : srv->lanes) {
+      if (ln.inflight != 0 || ln.arena_bytes >= bytes_per_lane) continue;
+      cudaError_t e = ln.arena ? cudaFreeAsync(ln.arena, ln.stream) : cudaSuccess;
+      srv->in_use -= ln.arena_bytes;
+      ln.arena = nullptr;
+      ln.arena_bytes = 0;
+      if (e == cudaSuccess) e = cudaMallocAsync(&ln.arena, bytes_per_lane, ln.stream);
+      if (e != cudaSuccess) {
+        ln.arena = nullptr;
+        g_server_error = std::string("CUDA: lane arena: ") + cudaGetErrorString(e);
+        return NTT_B200_ERR_CUDA;
+      }
+      ln.arena_bytes = bytes_per_lane;
+      srv->in_use += bytes_per_lane;
+    }
+    srv->peak_in_use = std::max(srv->peak_in_use, srv->in_use);
     return NTT_B200_OK;
   });
 }

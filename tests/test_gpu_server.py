@@ -48,11 +48,15 @@ def _check(orc, cases):
         np.testing.assert_array_equal(nb.to_host(c.out_a), wa, err_msg=f"{c.kind} N={ctx.n} L={c.level}")
 
 
-@pytest.mark.parametrize("lanes,depth,max_batch", [(3, 1, 8), (1, 2, 1), (2, 3, 4)])
-def test_served_results_equal_oracle_under_concurrent_arrivals(lib, orc, lanes, depth, max_batch):
+# (lanes, depth, max_batch, max_inflight_bytes): a cap of 1 byte lets only one
+# wave run at a time (and must never stall); 64 MB admits several small waves.
+@pytest.mark.parametrize("lanes,depth,max_batch,cap", [(3, 1, 8, 0), (1, 2, 1, 0), (2, 3, 4, 0), (4, 2, 8, 1),
+                                                       (4, 2, 16, 64 << 20)])
+def test_served_results_equal_oracle_under_concurrent_arrivals(lib, orc, lanes, depth, max_batch, cap):
     contexts = _contexts(orc)
-    cases = _random_cases(orc, contexts, 48, 7 + lanes)
-    srv = nb.Server(device=0, lanes=lanes, max_batch=max_batch, hbm_budget_bytes=2 << 30, depth=depth)
+    cases = _random_cases(orc, contexts, 48, 7 + lanes + cap % 97)
+    srv = nb.Server(device=0, lanes=lanes, max_batch=max_batch, hbm_budget_bytes=2 << 30, depth=depth,
+                    max_inflight_bytes=cap)
     tickets = {}
 
     def producer(part, delay_s):
@@ -84,7 +88,7 @@ def test_arrivals_during_running_waves_join_later_waves(lib, orc):
     keys = _keys(orc, ctx, 5)
     first = [Case(orc, ctx, 12, 100 + i, keys, "switch") for i in range(16)]
     later = [Case(orc, ctx, 12, 200 + i, keys, "rotate", 5) for i in range(16)]
-    srv = nb.Server(device=0, lanes=2, max_batch=4, hbm_budget_bytes=4 << 30)
+    srv = nb.Server(device=0, lanes=2, max_batch=4, hbm_budget_bytes=4 << 30, depth=1, max_inflight_bytes=0)
     t1 = [srv.submit(g, c.request()) for c in first]
     t2 = [srv.submit(g, c.request()) for c in later]
     info = [srv.wait(t) for t in t1 + t2]
@@ -133,3 +137,24 @@ def test_submission_contract_errors(lib, orc):
         srv.wait(t)  # already collected
     srv.close()
     _check(orc, [(ctx, g, c)])
+
+
+def test_reserve_sizes_idle_arenas_within_the_budget(lib, orc):
+    ctx = synthetic_context(orc, 8192, 6, 3, 2)
+    g = nb.Context.from_oracle(ctx)
+    keys = _keys(orc, ctx, 11)
+    cases = [Case(orc, ctx, 6, 400 + i, keys, "switch") for i in range(6)]
+    one = g.requests_workspace_bytes([cases[0].request()])
+    srv = nb.Server(device=0, lanes=3, max_batch=1, hbm_budget_bytes=3 * one, depth=1, max_inflight_bytes=0)
+    srv.reserve(one)
+    assert srv.stats()["in_flight_bytes"] == 3 * one
+    with pytest.raises(nb.ContractError):
+        srv.reserve(one + 1)  # three lanes would exceed the budget
+    srv.reserve(one)  # already that large: nothing to do
+    tickets = [srv.submit(g, c.request()) for c in cases]
+    info = [srv.wait(t) for t in tickets]
+    stats = srv.stats()
+    srv.close()
+    _check(orc, [(ctx, g, c) for c in cases])
+    assert all(i.status == nb.OK for i in info)
+    assert stats["peak_bytes"] == 3 * one  # the reserved arenas carried every wave
