@@ -197,7 +197,9 @@ int ntt_b200_keyswitch_requests_workspace(ntt_b200_context ctx, const ntt_b200_k
                                           size_t count, size_t *bytes);
 /* Key switch a list of requests of mixed levels, keys, rotations and
  * relinearization addends. Requests are grouped by level (shape class) and
- * each group of up to 128 runs as one pass of the fused pipeline; each result
+ * each group of up to 128 runs as one pass of the fused pipeline; the level
+ * groups run concurrently on up to four streams forked from `stream` and
+ * joined back into it (each with its own part of the workspace); each result
  * equals the request run alone. Outputs must not overlap any other buffer of
  * the call (except a request's own addend at the same address). The reference
  * has no batch API: per request this equals its Session chain

@@ -181,6 +181,10 @@ struct HostConvPlan {
 };
 }  // namespace
 
+// Streams a request-list call spreads its level groups over: the caller's
+// stream plus kChunkLanes - 1 side streams forked from it and joined back.
+constexpr size_t kChunkLanes = 4;
+
 struct ntt_b200_context_s {
   int device = 0;
   u64 n = 0;
@@ -204,6 +208,14 @@ struct ntt_b200_context_s {
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
   cudaEvent_t ev_start = nullptr;
   std::mutex pipe_mu;
+  // Request lists whose requests span several levels run one level group per
+  // stream: side streams forked from the caller's stream by ev_fork and joined
+  // back by ev_join. Created by ntt_b200_context_prepare (so capture never
+  // creates them) or on first use; chunk_mu keeps each call's event records
+  // and waits paired when several host threads share the context.
+  cudaStream_t side[kChunkLanes - 1] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kChunkLanes - 1] = {};
+  std::mutex chunk_mu;
 
   size_t towers() const { return m + k; }
 
@@ -221,6 +233,11 @@ struct ntt_b200_context_s {
     if (copy_out) cudaStreamDestroy(copy_out);
     for (cudaEvent_t e : {ev_in[0], ev_in[1], ev_comp[0], ev_comp[1], ev_out[0], ev_out[1], ev_start})
       if (e) cudaEventDestroy(e);
+    for (cudaStream_t s : side)
+      if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : ev_join)
+      if (e) cudaEventDestroy(e);
+    if (ev_fork) cudaEventDestroy(ev_fork);
     cudaFree(d_tc);
     cudaFree(d_fwd);
     cudaFree(d_inv);
@@ -1222,10 +1239,64 @@ void validate_requests(const Ctx &c, const ntt_b200_ks_request *reqs, size_t cou
   }
 }
 
+// Streams for a call's chunks. Chunks of one level stay on one stream, in call
+// order, and share its workspace region; the level groups are spread over up
+// to kChunkLanes streams, largest first onto the least-loaded stream, so small
+// groups fill the GPU beside large ones instead of running one after another.
+// Region l is the largest chunk of lane l; the regions lie back to back.
+struct LanePlan {
+  std::vector<std::vector<size_t>> lanes;  // chunk indices per stream, lane 0 = the caller's
+  std::vector<size_t> region;              // workspace bytes per stream
+};
+
+LanePlan plan_lanes(const Ctx &c, const std::vector<Chunk> &chunks) {
+  std::vector<size_t> levels;
+  std::vector<std::vector<size_t>> groups;
+  for (size_t i = 0; i < chunks.size(); ++i) {
+    const auto it = std::find(levels.begin(), levels.end(), chunks[i].level);
+    if (it == levels.end()) {
+      levels.push_back(chunks[i].level);
+      groups.push_back({i});
+    } else {
+      groups[size_t(it - levels.begin())].push_back(i);
+    }
+  }
+  std::vector<size_t> work(groups.size(), 0), order(groups.size());
+  for (size_t g = 0; g < groups.size(); ++g) {
+    for (size_t i : groups[g]) work[g] += chunk_bytes(c, chunks[i]);
+    order[g] = g;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return work[a] > work[b]; });
+  LanePlan p;
+  const size_t nl = std::min(groups.size(), kChunkLanes);
+  p.lanes.resize(nl);
+  p.region.assign(nl, 0);
+  std::vector<size_t> load(nl, 0);
+  for (size_t g : order) {
+    const size_t l = size_t(std::min_element(load.begin(), load.end()) - load.begin());
+    load[l] += work[g];
+    for (size_t i : groups[g]) {
+      p.lanes[l].push_back(i);
+      p.region[l] = std::max(p.region[l], chunk_bytes(c, chunks[i]));
+    }
+  }
+  for (auto &lane : p.lanes) std::sort(lane.begin(), lane.end());
+  return p;
+}
+
 size_t requests_bytes(const Ctx &c, const std::vector<Chunk> &chunks) {
   size_t need = 0;
-  for (const Chunk &ch : chunks) need = std::max(need, chunk_bytes(c, ch));
+  for (size_t r : plan_lanes(c, chunks).region) need += r;
   return need;
+}
+
+// Side streams and fork/join events of the request-list path (chunk_mu held).
+void ensure_chunk_lanes(Ctx &c) {
+  if (c.ev_fork) return;
+  DeviceGuard guard(c.device);
+  for (auto &s : c.side) CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  for (auto &e : c.ev_join) CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
 }
 }  // namespace
 
@@ -1463,6 +1534,8 @@ int ntt_b200_context_prepare(ntt_b200_context ctx, size_t level) {
         if (t < first || t >= first + count) tgt.push_back(all[t]);
       for (const bool ninv : {false, true}) c.conv_plan(range_ids(first, first + count), tgt, ninv);
     }
+    std::lock_guard<std::mutex> lock(c.chunk_mu);
+    ensure_chunk_lanes(c);
   });
 }
 
@@ -1709,10 +1782,44 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
       c.down_plan(ch.level);
     }
     const cudaStream_t st = as_stream(stream);
-    for (const Chunk &ch : chunks) {
-      // Chunks run in stream order, so each reuses the same workspace.
-      Carver ws{reinterpret_cast<char *>(workspace), workspace_bytes};
-      run_chunk(c, reqs, ch, ws, st);
+    const LanePlan plan = plan_lanes(c, chunks);
+    char *const base = reinterpret_cast<char *>(workspace);
+    if (plan.lanes.size() == 1) {
+      for (size_t i : plan.lanes[0]) {
+        // Chunks run in stream order, so each reuses the same workspace.
+        Carver ws{base, plan.region[0]};
+        run_chunk(c, reqs, chunks[i], ws, st);
+      }
+      return;
+    }
+    std::lock_guard<std::mutex> lock(c.chunk_mu);
+    ensure_chunk_lanes(c);
+    CUDA_CHECK(cudaEventRecord(c.ev_fork, st));
+    // Every forked stream is joined back into the caller's stream, also when an
+    // enqueue fails part way, so no side-stream work outlives the call's stream.
+    struct Join {
+      Ctx &c;
+      cudaStream_t st;
+      size_t forked = 0;
+      ~Join() {
+        for (size_t l = 0; l < forked; ++l) {
+          cudaEventRecord(c.ev_join[l], c.side[l]);
+          cudaStreamWaitEvent(st, c.ev_join[l], 0);
+        }
+      }
+    } join{c, st};
+    size_t off = 0;
+    for (size_t l = 0; l < plan.lanes.size(); ++l) {
+      const cudaStream_t ls = l == 0 ? st : c.side[l - 1];
+      if (l > 0) {
+        CUDA_CHECK(cudaStreamWaitEvent(ls, c.ev_fork, 0));
+        join.forked = l;
+      }
+      for (size_t i : plan.lanes[l]) {
+        Carver ws{base + off, plan.region[l]};
+        run_chunk(c, reqs, chunks[i], ws, ls);
+      }
+      off += plan.region[l];
     }
   });
 }
