@@ -466,6 +466,7 @@ Tunable g_tuning[] = {
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
     {"mac_approx", {1}, 0, 1},         // MAC reductions with approximate quotients (moduli below 2^61)
     {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
+    {"mac_rotate", {0}, 0, 1},         // key-switch rotations fused into the MAC's stores (else a gather pass)
     {"conv_tc", {1}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
     {"conv_tc_tiles", {4}, 1, 16},     // 128-coefficient tiles per tensor-core conversion CTA
@@ -943,15 +944,42 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
 
 // MAC of `polys` requests: out_b/out_a of request z at out + z * out_stride;
 // digit d of request z at digits[d] + z * digit_poly_stride.
+bool mac_limbs_apply(const Ctx &c) {
+  u64 max_q = 0;
+  for (auto q : c.mod) max_q = std::max(max_q, q);
+  return max_q < (u64(1) << 60) && tuned("mac_limbs") != 0;
+}
+
+// Whether a key switch at level L rotates inside the MAC (mac2_kernel's ROT
+// form: two coefficients per thread, at most 4 digits) instead of a separate
+// rotate_kernel pass over the extended result.
+bool mac_fuses_rotation(const Ctx &c, size_t L) {
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  return tuned("mac_rotate") != 0 && c.n >= 2 * (u64)b200::kEwThreads && beta <= 4 && !mac_limbs_apply(c);
+}
+
+// Rotation fused into the MAC: c0 of request z at c0 + z * c0_stride (request
+// tables carry their own c0 and automorphism).
+struct MacRotation {
+  bool on = false;
+  const u64 *c0 = nullptr;
+  u64 c0_stride = 0;
+  uint32_t g = 1;
+};
+
 void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride,
             const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
             const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a, bool full_key_rows,
-            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr, bool lazy_digits = false) {
+            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr, bool lazy_digits = false,
+            const MacRotation &rot = {}) {
   const size_t n = c.n, T = L + c.k;
   const size_t beta = digits.size();
   require(beta >= 1 && beta <= (size_t)b200::kMaxDigits &&
               (req || (key_b.size() == beta && key_a.size() == beta)),
           "MAC digit count out of range");
+  require(!rot.on || (mac_fuses_rotation(c, L) && beta == 1 + (L - 1) / c.alpha && !accumulate),
+          "rotation fused into the MAC needs its two-coefficient form and no accumulation");
+  require(req || !rot.on || ((rot.g & 1) && rot.g < 2 * c.n), "invalid negacyclic automorphism index");
   b200::MacArgs a{};
   a.out_b = out_b;
   a.out_a = out_a;
@@ -976,12 +1004,18 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
   a.logn = c.logn;
   a.full_key_rows = full_key_rows;
   a.accumulate = accumulate;
+  if (rot.on) {
+    a.c0 = rot.c0;
+    a.c0_poly_stride = rot.c0_stride;
+    a.g = rot.g;
+    a.plan = c.down_plan(L);
+  }
   u64 max_q = 0;
   for (auto q : c.mod) max_q = std::max(max_q, q);
   // Lazy digits lie in [0, 8q).
   const u128 prod = (u128)(lazy_digits ? 8 * max_q - 1 : max_q - 1) * (max_q - 1);
   const bool wide = prod > (~(u128)0) / (u128)beta;
-  const bool limbs = max_q < (u64(1) << 60) && tuned("mac_limbs") != 0;
+  const bool limbs = mac_limbs_apply(c);
   require(!lazy_digits || (!limbs && beta <= 4 && n >= 2 * b200::kEwThreads), "lazy digits need the 2-coefficient MAC");
   Timed t("mac", st);
   if (n >= 2 * b200::kEwThreads && beta <= 4 && limbs) {
@@ -996,12 +1030,21 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
     const dim3 grid2((unsigned)(n / (2 * b200::kEwThreads)), (unsigned)polys, (unsigned)T);
     auto launch = [&](auto beta_tag) {
       constexpr int B = decltype(beta_tag)::value;
-      if (wide)
+      const bool approx = !wide && c.mode == 2 && tuned("mac_approx");  // every modulus below 2^61
+      if (rot.on) {
+        if (wide)
+          b200::mac2_kernel<B, true, false, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
+        else if (approx)
+          b200::mac2_kernel<B, false, true, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
+        else
+          b200::mac2_kernel<B, false, false, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
+      } else if (wide) {
         b200::mac2_kernel<B, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
-      else if (c.mode == 2 && tuned("mac_approx"))  // every modulus below 2^61
+      } else if (approx) {
         b200::mac2_kernel<B, false, true><<<grid2, b200::kEwThreads, 0, st>>>(a);
-      else
+      } else {
         b200::mac2_kernel<B, false><<<grid2, b200::kEwThreads, 0, st>>>(a);
+      }
     };
     switch (beta) {
       case 1: launch(std::integral_constant<int, 1>{}); break;
@@ -1060,13 +1103,15 @@ void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const 
   u64 *acc = ws.take(2 * batch * T * n);  // [batch][b|a][T][N]
   u64 *rot = ws.take(2 * batch * T * n);
   const bool lazy = digits_lazy(c, beta);
+  const bool fused = c0 && mac_fuses_rotation(c, L);
+  if (c0) require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
   do_digits(c, L, batch, digits, src, ws, false, st, nullptr, lazy);
   std::vector<const u64 *> dptr;
   for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
   do_mac(c, L, batch, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, src, key_digits(c, key_b, beta),
-         key_digits(c, key_a, beta), true, false, st, nullptr, lazy);
+         key_digits(c, key_a, beta), true, false, st, nullptr, lazy, MacRotation{fused, c0, L * n, g});
   const u64 *ext = acc;
-  if (c0) {
+  if (c0 && !fused) {
     do_rotate(c, L, batch, rot, rot + T * n, acc, acc + T * n, 2 * T * n, c0, L * n, g, st);
     ext = rot;
   }
@@ -1128,7 +1173,7 @@ size_t chunk_bytes(const Ctx &c, const Chunk &ch) {
   const size_t n = c.n, L = ch.level, K = c.k, T = L + K, r = ch.idx.size(), u = ch.usrc.size();
   const size_t beta = 1 + (L - 1) / c.alpha;
   return aligned_bytes(table_words(r, u)) + aligned_bytes(u * beta * T * n) + aligned_bytes(u * L * n) +
-         aligned_bytes(2 * r * T * n) + (ch.rotate ? aligned_bytes(2 * r * T * n) : 0) +
+         aligned_bytes(2 * r * T * n) + (ch.rotate && !mac_fuses_rotation(c, L) ? aligned_bytes(2 * r * T * n) : 0) +
          aligned_bytes(2 * r * K * n) + aligned_bytes(2 * r * L * n);
 }
 
@@ -1182,14 +1227,16 @@ void run_chunk(Ctx &c, const ntt_b200_ks_request *reqs, const Chunk &ch, Carver 
 
   u64 *digits = ws.take(u * beta * T * n);
   u64 *acc = ws.take(2 * r * T * n);  // [request][b|a][T][N]
-  u64 *rot = ch.rotate ? ws.take(2 * r * T * n) : nullptr;
+  const bool fused = ch.rotate && mac_fuses_rotation(c, L);
+  u64 *rot = ch.rotate && !fused ? ws.take(2 * r * T * n) : nullptr;
   const bool lazy = digits_lazy(c, beta);
   do_digits(c, L, u, digits, nullptr, ws, false, st, usrc, lazy);
   std::vector<const u64 *> dptr;
   for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
-  do_mac(c, L, r, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, nullptr, {}, {}, true, false, st, desc, lazy);
+  do_mac(c, L, r, acc, acc + T * n, 2 * T * n, dptr, beta * T * n, nullptr, {}, {}, true, false, st, desc, lazy,
+         MacRotation{fused});
   const u64 *ext = acc;
-  if (ch.rotate) {
+  if (ch.rotate && !fused) {
     do_rotate(c, L, r, rot, rot + T * n, acc, acc + T * n, 2 * T * n, nullptr, 0, 1, st, desc);
     ext = rot;
   }

@@ -457,6 +457,25 @@ constexpr int kMaxDigits = 40;
 
 // One key-switch request of a request-table launch (a device-resident table
 // written by put_words before the pipeline runs).
+// Evaluation-domain automorphism X -> X^g on the bit-reversed layout: output
+// slot k takes input slot automorphism_source(k) (automorphism_source_index of
+// include/ntt/resident_conversion.hpp:15-29; resident_adapter.inc:44-59).
+__device__ __forceinline__ uint32_t automorphism_source(uint32_t k, int logn, uint32_t g) {
+  const uint32_t odd = 2 * (__brev(k) >> (32 - logn)) + 1;
+  const uint32_t src = (uint32_t)((u64(odd) * g) & ((u64(2) << logn) - 1));
+  return __brev(src >> 1) >> (32 - logn);
+}
+// g^-1 mod 2^32 for odd g by Newton's iteration x <- x(2 - gx), which doubles
+// the correct low bits (g*g = 1 mod 8 gives 3 to start: 6, 12, 24, 48). Input
+// slot i of the automorphism by g lands in output slot automorphism_source(i)
+// of g^-1, since (2 bitrev(i) + 1) g^-1 undoes the multiplication by g.
+__device__ __forceinline__ uint32_t inverse_mod_pow2(uint32_t g) {
+  uint32_t x = g;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) x *= 2u - g * x;
+  return x;
+}
+
 struct ReqDesc {
   const u64 *src;            // evaluation Q_L component being switched ([L][N])
   const u64 *key_b, *key_a;  // full-context key: digit d at key + d * key_digit_stride
@@ -478,6 +497,13 @@ struct MacArgs {
   u64 poly_stride_out, poly_stride_digits, poly_stride_input;
   int level, m, beta, alpha, logn;
   bool full_key_rows, accumulate;
+  // Rotation fused into the MAC (mac2_kernel<..., ROT>): request z adds P * c0
+  // on its Q towers of the b channel and writes slot i to automorphism slot
+  // automorphism_source(i, g^-1). Request-table mode takes c0 and g from req[z].
+  const u64 *c0;
+  u64 c0_poly_stride;
+  const DownPlan *plan;  // the level's P mod q_i
+  uint32_t g;
 };
 
 // Per-request bases of a MAC thread: request z's digit slot, input and keys.
@@ -485,6 +511,8 @@ struct MacBases {
   u64 dz;
   const u64 *input;
   const u64 *kb, *ka;  // request-table mode: digit 0 of the request's key
+  const u64 *c0;       // rotation: the request's c0 (null: none)
+  uint32_t g;          // rotation: the request's automorphism (1: identity)
 };
 __device__ __forceinline__ MacBases mac_bases(const MacArgs &a, u64 z) {
   MacBases m;
@@ -494,10 +522,14 @@ __device__ __forceinline__ MacBases mac_bases(const MacArgs &a, u64 z) {
     m.input = r.src;
     m.kb = r.key_b;
     m.ka = r.key_a;
+    m.c0 = r.c0;
+    m.g = r.g;
   } else {
     m.dz = z;
     m.input = a.input ? a.input + z * a.poly_stride_input : nullptr;
     m.kb = m.ka = nullptr;
+    m.c0 = a.c0 ? a.c0 + z * a.c0_poly_stride : nullptr;
+    m.g = a.g;
   }
   return m;
 }
@@ -541,7 +573,12 @@ __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
 // thread (16-byte loads of every digit and key row).
 // APPROX (every modulus below 2^61, sums below 2^128): the final reductions
 // take approximate quotients (reduce128_approx); results are identical.
-template <int BETA, bool WIDE, bool APPROX = false>
+// ROT: the rotation of the extended result (rotate_kernel) happens here: the
+// sums at slot i, plus P * c0[i] on the b channel's Q towers, are stored at
+// the slot that the automorphism moves i to. That saves the rotation's full
+// read and write of both QP channels; the stores are 8-byte scattered ones
+// within a tower, which L2 merges before they reach HBM. Not with accumulate.
+template <int BETA, bool WIDE, bool APPROX = false, bool ROT = false>
 __global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
   static_assert(!(WIDE && APPROX), "approximate reduction needs sums below 2^128");
   const u64 n = u64(1) << a.logn;
@@ -582,6 +619,23 @@ __global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
     rb.y = reduce(b1, red);
     ra.x = reduce(a0, red);
     ra.y = reduce(a1, red);
+  }
+  if constexpr (ROT) {
+    if (mb.c0 && t < a.level) {  // rotated_b_value: b + P * c0 on the Q towers
+      const Shoup pm = a.plan->p_mod[t];
+      const ulonglong2 c = *reinterpret_cast<const ulonglong2 *>(mb.c0 + t * n + i);
+      rb.x = add_mod(rb.x, shoup_canon(c.x, pm.w, pm.wq, red.m), red.m);
+      rb.y = add_mod(rb.y, shoup_canon(c.y, pm.w, pm.wq, red.m), red.m);
+    }
+    const uint32_t gi = inverse_mod_pow2(mb.g);
+    const u64 base = o - i;
+    const u64 d0 = base + automorphism_source((uint32_t)i, a.logn, gi);
+    const u64 d1 = base + automorphism_source((uint32_t)i + 1, a.logn, gi);
+    a.out_b[d0] = rb.x;
+    a.out_b[d1] = rb.y;
+    a.out_a[d0] = ra.x;
+    a.out_a[d1] = ra.y;
+    return;
   }
   if (a.accumulate) {
     const ulonglong2 ob = *reinterpret_cast<const ulonglong2 *>(a.out_b + o);
@@ -658,13 +712,6 @@ __global__ void __launch_bounds__(kEwThreads) mac2_limb_kernel(MacArgs a) {
 }
 
 // ---- rotation: automorphism gather plus P*c0 on Q towers ------------------------
-// resident_adapter.inc:44-59 semantics with automorphism_source_index and
-// rotated_b_value (resident_conversion.hpp:15-29).
-__device__ __forceinline__ uint32_t automorphism_source(uint32_t k, int logn, uint32_t g) {
-  const uint32_t odd = 2 * (__brev(k) >> (32 - logn)) + 1;
-  const uint32_t src = (uint32_t)((u64(odd) * g) & ((u64(2) << logn) - 1));
-  return __brev(src >> 1) >> (32 - logn);
-}
 // With a request table, request z rotates by req[z].g and adds P * req[z].c0
 // (a request without c0 and g = 1 passes through unchanged).
 struct RotateArgs {
