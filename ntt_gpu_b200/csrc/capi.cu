@@ -466,7 +466,7 @@ Tunable g_tuning[] = {
     {"conv_limbs", {1}, 0, 1},         // 30-bit-limb conversion kernel where it applies
     {"mac_approx", {1}, 0, 1},         // MAC reductions with approximate quotients (moduli below 2^61)
     {"mac_limbs", {0}, 0, 1},          // 30-bit-limb MAC kernel where it applies (slower on B200: off)
-    {"mac_rotate", {0}, 0, 1},         // key-switch rotations fused into the MAC's stores (else a gather pass)
+    {"mac_rotate", {1}, 0, 1},         // key-switch rotations fused into the MAC's stores (else a gather pass)
     {"conv_tc", {1}, 0, 1},            // tensor-core (tcgen05, int8 limbs) conversion where it applies
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
     {"conv_tc_tiles", {4}, 1, 16},     // 128-coefficient tiles per tensor-core conversion CTA
