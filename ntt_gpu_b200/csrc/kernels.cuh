@@ -578,8 +578,12 @@ __global__ void __launch_bounds__(kEwThreads) mac_kernel(MacArgs a) {
 // the slot that the automorphism moves i to. That saves the rotation's full
 // read and write of both QP channels; the stores are 8-byte scattered ones
 // within a tower, which L2 merges before they reach HBM. Not with accumulate.
+// Resident CTAs per SM: 5 (48 registers), 6 with the rotation (40). The MAC
+// waits mostly on its loads, and the extra warps cut its time by 5% and 10%
+// on a B200 (16 requests at L = 24) against the unconstrained 52 registers,
+// despite a few bytes of spills.
 template <int BETA, bool WIDE, bool APPROX = false, bool ROT = false>
-__global__ void __launch_bounds__(kEwThreads) mac2_kernel(MacArgs a) {
+__global__ void __launch_bounds__(kEwThreads, ROT ? 6 : 5) mac2_kernel(MacArgs a) {
   static_assert(!(WIDE && APPROX), "approximate reduction needs sums below 2^128");
   const u64 n = u64(1) << a.logn;
   const u64 i = (u64(blockIdx.x) * blockDim.x + threadIdx.x) * 2;
