@@ -11,12 +11,16 @@
 //  - acquire() makes the key resident in HBM (a stream-ordered allocation and
 //    upload on the caller's stream), evicting least-recently-used eligible
 //    keys to stay within the budget, pins it and returns its device pointers;
-//  - release() unpins it in stream order: an event recorded on the caller's
-//    stream must complete before the key becomes eligible for eviction, so
-//    work already enqueued never loses its key;
+//  - a key acquired on another stream than the one that uploaded it makes that
+//    stream wait for the upload (an event recorded after the copy), so no
+//    caller reads a key whose upload is still in flight;
+//  - release() unpins it in stream order: every release records its own event
+//    on the caller's stream, and the key becomes eligible for eviction only
+//    once all of them have completed, so work already enqueued on any stream
+//    never loses its key;
 //  - eviction frees device memory stream-ordered on the cache's own stream,
-//    once the key's last release event has completed (the callers' streams may
-//    be gone by then).
+//    after the host has seen every release event of the key complete (the
+//    callers' streams may be gone by then).
 // A key is identified by a caller-chosen 64-bit id (the reference's
 // EvaluationKeyCacheKey material token plus kind and index).
 #include <cuda_runtime.h>
@@ -49,7 +53,9 @@ struct Entry {
   uint64_t *host = nullptr;     // pinned: [b | a]
   uint64_t *dev = nullptr;      // resident copy [b | a], or null
   int pins = 0;
-  cudaEvent_t released = nullptr;  // last release point; eligible once it has completed
+  cudaEvent_t uploaded = nullptr;       // recorded after the upload of the resident copy
+  cudaStream_t upload_stream = nullptr;  // the stream that upload was enqueued on
+  std::vector<cudaEvent_t> releases;     // release points not yet seen complete, one per release
   std::list<uint64_t>::iterator lru;  // position in the resident LRU list
 };
 }  // namespace
@@ -63,11 +69,40 @@ struct ntt_b200_keycache_s {
   std::unordered_map<uint64_t, Entry> entries;
   std::list<uint64_t> lru;  // resident keys, most recently used at the front
 
+  std::vector<cudaEvent_t> spare;  // completed release events, reused by later releases
+
   size_t bytes(const Entry &e) const { return 2 * e.words * sizeof(uint64_t); }
 
-  bool eligible(const Entry &e) const {
+  // Drops the release events of `e` that have completed (back to the spare
+  // pool); true when none is left pending.
+  bool settled(Entry &e) {
+    auto pending = e.releases.begin();
+    for (cudaEvent_t ev : e.releases) {
+      if (cudaEventQuery(ev) == cudaSuccess)
+        spare.push_back(ev);
+      else
+        *pending++ = ev;
+    }
+    e.releases.erase(pending, e.releases.end());
+    return e.releases.empty();
+  }
+
+  // Resident, unpinned, and every stream that released it has passed its
+  // release point: no enqueued work reads it any more.
+  bool eligible(Entry &e) {
     if (!e.dev || e.pins > 0) return false;
-    return !e.released || cudaEventQuery(e.released) == cudaSuccess;
+    // A release on another stream than the upload's does not order after it.
+    if (e.uploaded && cudaEventQuery(e.uploaded) != cudaSuccess) return false;
+    return settled(e);
+  }
+
+  cudaError_t take_event(cudaEvent_t *ev) {
+    if (!spare.empty()) {
+      *ev = spare.back();
+      spare.pop_back();
+      return cudaSuccess;
+    }
+    return cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   }
 
   // Evict one entry (lock held; the entry is eligible).
@@ -100,9 +135,9 @@ struct ntt_b200_keycache_s {
                                             "key cache budget exhausted by pinned or in-use keys");
   }
 
-  size_t pinned_bytes() const {
+  size_t pinned_bytes() {
     size_t p = 0;
-    for (const auto &kv : entries)
+    for (auto &kv : entries)
       if (kv.second.dev && (kv.second.pins > 0 || !eligible(kv.second))) p += bytes(kv.second);
     return p;
   }
@@ -162,6 +197,12 @@ int ntt_b200_keycache_acquire(ntt_b200_keycache c, uint64_t key_id, void *stream
   if (e.dev) {
     c->hits += 1;
     c->lru.erase(e.lru);
+    // The upload may still be in flight on the stream that made the key
+    // resident: a caller on another stream waits for it.
+    if (e.uploaded && st != e.upload_stream) {
+      const cudaError_t err = cudaStreamWaitEvent(st, e.uploaded, 0);
+      if (err != cudaSuccess) rc = cuda_fail(err, "cudaStreamWaitEvent");
+    }
   } else {
     c->misses += 1;
     const size_t need = c->bytes(e);
@@ -169,13 +210,17 @@ int ntt_b200_keycache_acquire(ntt_b200_keycache c, uint64_t key_id, void *stream
                           : c->make_room(need, c->budget);
     if (rc == NTT_B200_OK) {
       void *dev = nullptr;
-      cudaError_t err = cudaMallocAsync(&dev, need, st);
+      cudaError_t err = cudaSuccess;
+      if (!e.uploaded) err = cudaEventCreateWithFlags(&e.uploaded, cudaEventDisableTiming);
+      if (err == cudaSuccess) err = cudaMallocAsync(&dev, need, st);
       if (err == cudaSuccess) err = cudaMemcpyAsync(dev, e.host, need, cudaMemcpyHostToDevice, st);
+      if (err == cudaSuccess) err = cudaEventRecord(e.uploaded, st);
       if (err != cudaSuccess) {
         if (dev) cudaFreeAsync(dev, st);
         rc = cuda_fail(err, "key upload");
       } else {
         e.dev = static_cast<uint64_t *>(dev);
+        e.upload_stream = st;
         c->allocated += need;
       }
     }
@@ -200,11 +245,17 @@ int ntt_b200_keycache_release(ntt_b200_keycache c, uint64_t key_id, void *stream
   int previous = 0;
   cudaGetDevice(&previous);
   if (previous != c->device) cudaSetDevice(c->device);
-  cudaError_t err = cudaSuccess;
-  if (!e.released) err = cudaEventCreateWithFlags(&e.released, cudaEventDisableTiming);
-  if (err == cudaSuccess) err = cudaEventRecord(e.released, reinterpret_cast<cudaStream_t>(stream));
+  // One event per release: releases on different streams are all waited for
+  // before the key can be evicted and its memory freed.
+  cudaEvent_t ev = nullptr;
+  cudaError_t err = c->take_event(&ev);
+  if (err == cudaSuccess) err = cudaEventRecord(ev, reinterpret_cast<cudaStream_t>(stream));
   if (previous != c->device) cudaSetDevice(previous);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaEventRecord");
+  if (err != cudaSuccess) {
+    if (ev) c->spare.push_back(ev);
+    return cuda_fail(err, "cudaEventRecord");
+  }
+  e.releases.push_back(ev);
   e.pins -= 1;
   return NTT_B200_OK;
 }
@@ -267,11 +318,18 @@ int ntt_b200_keycache_destroy(ntt_b200_keycache c) {
     cudaSetDevice(c->device);
     for (auto &kv : c->entries) {
       Entry &e = kv.second;
-      if (e.released) cudaEventSynchronize(e.released);
+      for (cudaEvent_t ev : e.releases) {
+        cudaEventSynchronize(ev);
+        cudaEventDestroy(ev);
+      }
+      if (e.uploaded) {
+        cudaEventSynchronize(e.uploaded);
+        cudaEventDestroy(e.uploaded);
+      }
       if (e.dev) cudaFree(e.dev);
-      if (e.released) cudaEventDestroy(e.released);
       cudaFreeHost(e.host);
     }
+    for (cudaEvent_t ev : c->spare) cudaEventDestroy(ev);
     cudaStreamSynchronize(c->free_stream);
     cudaStreamDestroy(c->free_stream);
   }

@@ -1,9 +1,11 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 Run in a container that has the reference tree (minnow54426/ntt-gpu) at
-REF (default /root/reference) and oracle/_ref built (make -C oracle ref):
+REF (argument, else $NTT_REFERENCE_TREE, else ../reference beside this
+repository) and oracle/_ref built (make -C oracle ref):
 
-    python tests/golden/make_golden.py [REF]
+    python tests/golden/make_golden.py [REF]            # every fixture
+    python tests/golden/make_golden.py --config5 [REF]  # only the config-5 digests, merged
 
 Two sources, neither of them this repository's oracle:
   * ntt_n1024.npz, ntt_n64.npz - the reference's Python big-integer oracle
@@ -123,14 +125,51 @@ def full_size_digests(orc, ref):
     return d
 
 
+def config5_digests(orc, ref):
+    """Config 5's largest shapes (N = 65536, L = 32, dnum 2/3/4, K = alpha):
+    key switch, rotations by +-1 and +-64 steps, and a short-last-digit level,
+    from the compiled reference's Session + HostDriver chain."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    import golden_cases as gc
+    d = {}
+    for dnum in gc.CONFIG5_DNUM:
+        ctx = gc.config5_context(orc, dnum)
+        kb, ka = full_keys(orc, ctx, 300 + dnum)
+        for name, level, x, c0, g in gc.config5_cases(orc, dnum):
+            b, a = ref.keyswitch(ctx, level, x, kb, ka, c0, g)
+            d[name + "_b"], d[name + "_a"] = sha(b), sha(a)
+            print(name, flush=True)
+    return d
+
+
+def reference_root(argv):
+    if argv:
+        return argv[0]
+    return os.environ.get("NTT_REFERENCE_TREE", os.path.join(ROOT, "..", "reference"))
+
+
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    args = sys.argv[1:]
+    only5 = "--config5" in args
+    args = [a for a in args if a != "--config5"]
+    ref_root = reference_root(args)
     orc, ref = Oracle(), Reference()
+    path = os.path.join(HERE, "digests.json")
+    if only5:
+        with open(path) as f:
+            d = json.load(f)
+        d.update(config5_digests(orc, ref))
+        with open(path, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        print("config-5 digests merged into", path)
+        return
     np.savez_compressed(os.path.join(HERE, "ntt_n1024.npz"), **naive_fixture(ref_root, 1024, 3, 46, 1))
     np.savez_compressed(os.path.join(HERE, "ntt_n64.npz"), **naive_fixture(ref_root, 64, 3, 46, 1))
     np.savez_compressed(os.path.join(HERE, "chain_small.npz"), **chain_cases(orc, ref))
-    with open(os.path.join(HERE, "digests.json"), "w") as f:
-        json.dump(full_size_digests(orc, ref), f, indent=1, sort_keys=True)
+    d = full_size_digests(orc, ref)
+    d.update(config5_digests(orc, ref))
+    with open(path, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
     print("golden fixtures written to", HERE)
 
 

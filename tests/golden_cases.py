@@ -69,3 +69,38 @@ def ntt_cases(orc):
     for name, q, psi in [("find_primes60", q60, orc.find_psi(q60, n)),
                          ("openfhe_q0", 1152921504606584833, 18043022392882)]:
         yield name, q, psi, orc.lcg(n, [q], LCG_SEED)
+
+
+# Config 5's largest shapes: N = 65536, L = 32 Q towers, dnum in {2, 3, 4} with
+# K = alpha = ceil(32 / dnum) P towers (16 / 11 / 8), as the mixed serving
+# workload builds its contexts. dnum = 2 runs 16-source conversions.
+CONFIG5_DNUM = (2, 3, 4)
+CONFIG5_STEPS = (1, -1, 64, -64)
+
+
+def rotation_index(n: int, step: int) -> int:
+    """Generator-5 rotation group: 5^s mod 2N for s >= 0, (5^-1)^|s| otherwise."""
+    two_n = 2 * n
+    g = pow(5, abs(step), two_n)
+    return g if step >= 0 else pow(g, -1, two_n)
+
+
+def config5_context(orc, dnum):
+    alpha = -(-32 // dnum)
+    return synthetic_context(orc, 65536, 32, alpha, dnum)
+
+
+def config5_cases(orc, dnum):
+    """(name, level, x, c0, automorphism) of one config-5 context; keys are
+    full_keys(orc, ctx, 300 + dnum). Rotations share the input of the L = 32
+    key switch (one hoisted decomposition), and L = 17 leaves the last digit
+    short (17 = 16 + 1, 11 + 6, 8 + 8 + 1)."""
+    ctx = config5_context(orc, dnum)
+    x = orc.lcg(ctx.n, ctx.q, LCG_SEED + 50 + dnum)
+    c0 = orc.lcg(ctx.n, ctx.q, LCG_SEED + 60 + dnum)
+    yield f"c5_d{dnum}_L32_ks", 32, x, None, 0
+    for step in CONFIG5_STEPS:
+        tag = f"p{step}" if step > 0 else f"m{-step}"
+        yield f"c5_d{dnum}_L32_rot{tag}", 32, x, c0, rotation_index(ctx.n, step)
+    x17 = orc.lcg(ctx.n, ctx.q[:17], LCG_SEED + 70 + dnum)
+    yield f"c5_d{dnum}_L17_ks", 17, x17, None, 0

@@ -50,3 +50,14 @@ def test_full_size_keyswitch_digests_pinned(orc):
             continue
         b, a = orc.keyswitch(ctx, level, x, kb, ka, c0, g)
         assert gc.sha(b) == d[name + "_b"] and gc.sha(a) == d[name + "_a"], name
+
+
+def test_config5_sixteen_source_digest(orc):
+    """The oracle reproduces the reference's key switch at config 5's widest
+    conversion shape (N = 65536, L = 32, dnum = 2: K = alpha = 16)."""
+    d = gc.digests()
+    ctx = gc.config5_context(orc, 2)
+    kb, ka = gc.full_keys(orc, ctx, 302)
+    name, level, x, c0, g = next(iter(gc.config5_cases(orc, 2)))
+    b, a = orc.keyswitch(ctx, level, x, kb, ka, c0, g)
+    assert gc.sha(b) == d[name + "_b"] and gc.sha(a) == d[name + "_a"], name

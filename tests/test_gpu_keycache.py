@@ -127,3 +127,75 @@ def test_server_takes_keys_from_cache_with_eviction(lib, orc):
         np.testing.assert_array_equal(nb.to_host(oa), wa)
     cache.close()
     g.close()
+
+
+def test_cold_key_shared_by_waves_on_several_lanes(lib, orc):
+    """A key that is not resident is uploaded on the stream of the first wave
+    that needs it; waves on the other lanes that take it while that upload is
+    in flight wait for it (every result exact)."""
+    ctx = synthetic_context(orc, 16384, 12, 4, 3)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka = full_keys(orc, ctx, 77)
+    cache = nb.KeyCache(device=0, budget_bytes=1 << 30)
+    cache.insert(g, 9, kb, ka)
+    srv = nb.Server(device=0, lanes=4, max_batch=2, hbm_budget_bytes=2 << 30, depth=2)
+    srv.attach_keycache(cache)
+    cases = []
+    for r in range(16):
+        x = orc.lcg(ctx.n, ctx.q, 4100 + r)
+        dx = nb.to_device(x)
+        ob, oa = nb.empty((12, ctx.n)), nb.empty((12, ctx.n))
+        cases.append((x, dx, ob, oa))
+    import torch
+    torch.cuda.synchronize()
+    tickets = [srv.submit(g, nb.make_request(12, dx, ob, oa, key_id=9)) for x, dx, ob, oa in cases]
+    infos = [srv.wait(t) for t in tickets]
+    srv.close()
+    assert all(i.status == nb.OK for i in infos)
+    assert len({i.lane for i in infos}) > 1
+    st = cache.stats()
+    assert st["misses"] == 1 and st["hits"] >= 1
+    for x, dx, ob, oa in cases:
+        wb, wa = orc.keyswitch(ctx, 12, x, kb, ka)
+        np.testing.assert_array_equal(nb.to_host(ob), wb)
+        np.testing.assert_array_equal(nb.to_host(oa), wa)
+    cache.close()
+    g.close()
+
+
+def test_releases_on_two_streams_both_hold_the_key(lib, orc):
+    """A key pinned on two streams and released on both stays resident until
+    the work before each release has completed: a release on an idle stream
+    after one on a busy stream does not make it evictable."""
+    import torch
+    ctx = synthetic_context(orc, 65536, 24, 8, 3)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka = full_keys(orc, ctx, 31)
+    key_bytes = 2 * 8 * kb.size
+    cache = nb.KeyCache(device=0, budget_bytes=4 * key_bytes)
+    cache.insert(g, 1, kb, ka)
+    busy, idle = torch.cuda.Stream(), torch.cuda.Stream()
+    b, a = cache.acquire(1, stream=busy)
+    cache.acquire(1, stream=idle)
+    batch, level = 4, 24
+    src = nb.to_device(np.stack([orc.lcg(ctx.n, ctx.q, 10 + i) for i in range(batch)]))
+    ob, oa = nb.empty((batch, level, ctx.n)), nb.empty((batch, level, ctx.n))
+    ws = g.workspace(nb.OP_KEYSWITCH, level, batch)
+    busy.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(busy):
+        for _ in range(30):  # tens of milliseconds of work that reads the key
+            rc = nb.load().ntt_b200_keyswitch_batch(g._h, level, batch, ob.data_ptr(), oa.data_ptr(),
+                                                    src.data_ptr(), ctypes.c_void_p(b), ctypes.c_void_p(a), None,
+                                                    0, ws.data_ptr(), ws.numel() * 8, busy.cuda_stream)
+            nb._check(rc)
+    cache.release(1, stream=busy)
+    cache.release(1, stream=idle)
+    idle.synchronize()
+    assert cache.trim() == 0  # the busy stream still reads the key
+    busy.synchronize()
+    assert cache.trim() == key_bytes
+    want = orc.keyswitch(ctx, level, orc.lcg(ctx.n, ctx.q, 10), kb, ka)
+    np.testing.assert_array_equal(nb.to_host(ob[0]), want[0])
+    np.testing.assert_array_equal(nb.to_host(oa[0]), want[1])
+    cache.close()
+    g.close()
