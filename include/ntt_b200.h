@@ -392,7 +392,8 @@ int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, 
  * bracketed by CUDA events on its own stream. query() waits for the recorded
  * events and returns the launch count and summed device time of one kernel
  * class ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col",
- * "ntt_small", "conv", "mac", "rotate", "correct", "pointwise"). The external
+ * "ntt_small", "conv", "mac", "row_mac" (the digits' forward row pass fused
+ * with the key multiplication), "rotate", "correct", "pointwise", "table"). The external
  * clock protocol mirrors the reference's collect_elapsed
  * (include/ntt/measurement.hpp:41-58). */
 int ntt_b200_timing_enable(int on);

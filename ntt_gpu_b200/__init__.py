@@ -519,7 +519,7 @@ class KeyCache:
 
 
 KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col", "ntt_small", "conv", "mac",
-                  "rotate", "correct", "pointwise", "table")
+                  "row_mac", "rotate", "correct", "pointwise", "table")
 
 
 def butterfly_rate(device: int = 0) -> float:

@@ -1,8 +1,7 @@
 """Autotuner for the launch choices of libntt_b200 (one B200, CUDA events).
 
 Every tunable (ntt_b200_tuning_name) is a launch choice that never changes a
-result: the NTT pass variant (one CTA per tile, or persistent and double
-buffered), the register budget each NTT pass is compiled for (3 or 4 resident
+result: the register budget each NTT pass is compiled for (3 or 4 resident
 CTAs per SM), whether the row passes stage their twiddles in shared memory, the
 conversion kernel (tensor cores, 30-bit limbs or 128-bit accumulators), the MAC
 kernel and
@@ -79,13 +78,11 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
     def ks_step():
         kctx.keyswitch_batch(24, batch, ob, oa, xs, kb, ka, ws)
 
-    passes = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col")
     # tunable -> (candidates, workload, kernel classes whose device time decides it, tunables pinned
     # while it is measured). The CUDA-core conversion choices serve the plans the tensor-core form
     # does not take (more than 16 sources, moduli outside [2^48, 2^61)), so they are measured with it off.
     cuda_core_conv = {"conv_tc": 0}
     plan = [
-        ("ntt_persistent", (0, 1), ntt_step, passes, {}),
         ("ntt_minb_fwd_col", (3, 4), ntt_step, ("ntt_fwd_col",), {}),
         ("ntt_minb_fwd_row", (3, 4), ntt_step, ("ntt_fwd_row",), {}),
         ("ntt_minb_inv_row", (3, 4), ntt_step, ("ntt_inv_row",), {}),
@@ -104,6 +101,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("conv_tc", (0, 1), ks_step, ("conv",), {}),
         ("conv_tc_fixed", (0, 1), ks_step, ("conv",), {"conv_tc": 1}),
         ("conv_tc_tiles", (1, 2, 4, 8), ks_step, ("conv",), {"conv_tc": 1}),
+        ("row_mac", (0, 1), ks_step, ("ntt_fwd_row", "mac", "row_mac"), {}),
     ]
     measurements, choices = {}, {}
     for name, candidates, step, kernels, pinned in plan:

@@ -22,7 +22,8 @@
 #include "arith.cuh"
 #include "kernels.cuh"
 #include "ntt.cuh"
-#include "ntt_ps.cuh"
+#include "rowmac.cuh"
+#include "rowmac.h"
 #include "tables.cuh"
 
 using b200::u64;
@@ -451,7 +452,6 @@ struct Tunable {
   int64_t lo, hi;
 };
 Tunable g_tuning[] = {
-    {"ntt_persistent", {0}, 0, 1},     // persistent double-buffered NTT passes instead of one CTA per tile
     {"ntt_minb_fwd_col", {4}, 3, 4},   // CTAs per SM the forward column pass is compiled for
     {"ntt_minb_fwd_row", {4}, 3, 4},
     {"ntt_minb_inv_row", {4}, 3, 4},
@@ -471,6 +471,8 @@ Tunable g_tuning[] = {
     {"conv_blocks_per_sm", {8}, 1, 64}, // target conversion blocks per SM when splitting targets
     {"conv_tc_tiles", {4}, 1, 16},     // 128-coefficient tiles per tensor-core conversion CTA
     {"conv_tc_fixed", {1}, 0, 1},      // tensor-core conversion kernels compiled for 8 -> 24/16/8 towers
+    {"row_mac", {1}, 0, 1},            // key multiplication fused into the digits' forward row pass
+    {"row_mac_max_beta", {4}, 1, 4},   // largest digit count the fused row pass takes (shared memory per CTA grows with it)
 };
 Tunable *find_tunable(const char *name) {
   for (auto &t : g_tuning)
@@ -479,53 +481,23 @@ Tunable *find_tunable(const char *name) {
 }
 int64_t tuned(const char *name) { return find_tunable(name)->value.load(std::memory_order_relaxed); }
 
-// Persistent double-buffered passes (ntt_ps.cuh): grid = resident CTAs of the
-// device; per-device launch attributes are set once.
+// SM count of a device (cached).
 int device_sms(int device) {
   static int sms[64] = {0};
   if (device < 0 || device >= 64) throw ContractError("device ordinal out of range");
   if (!sms[device]) CUDA_CHECK(cudaDeviceGetAttribute(&sms[device], cudaDevAttrMultiProcessorCount, device));
   return sms[device];
 }
-template <class Kernel>
-unsigned persistent_grid(Kernel kernel, int smem, uint32_t total, int device, int *cache) {
-  if (!cache[device]) {
-    CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int per_sm = 0;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, b200::kNttThreads, smem));
-    cache[device] = std::max(1, per_sm);
-  }
-  const uint64_t resident = uint64_t(cache[device]) * device_sms(device);
-  return (unsigned)std::min<uint64_t>(total, resident);
-}
-bool persistent_enabled() { return tuned("ntt_persistent") != 0; }
 // An inverse NTT that only feeds a basis switch skips N^-1 (folded into the
 // switch's plan) when the two-pass kernels run it.
-bool intt_unscaled(const Ctx &c) { return c.logn >= 12 && !persistent_enabled() && tuned("intt_unscaled") != 0; }
+bool intt_unscaled(const Ctx &c) { return c.logn >= 12 && tuned("intt_unscaled") != 0; }
 // Hybrid digits that only feed the fused MAC stay in the forward NTT's lazy
 // range [0, 8q): with every modulus below 2^61 and at most 4 digits, the MAC's
 // 128-bit sums stay below 2^127 and its reductions give canonical results. The
 // 30-bit-limb MAC needs inputs below 2^60, so it rules this out.
 bool digits_lazy(const Ctx &c, size_t beta) {
-  return c.mode == 2 && beta <= 4 && c.logn >= 12 && !persistent_enabled() && tuned("digits_lazy") != 0 &&
+  return c.mode == 2 && beta <= 4 && c.logn >= 12 && tuned("digits_lazy") != 0 &&
          tuned("mac_limbs") == 0;
-}
-
-template <int LOGN, int MODE, bool INV>
-void launch_col_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
-  static int cache[64] = {0};
-  constexpr int smem = b200::col_smem_bytes<LOGN>();
-  const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
-  const unsigned grid = persistent_grid(b200::ntt_col_ps<LOGN, MODE, INV>, smem, total, c.device, cache);
-  b200::ntt_col_ps<LOGN, MODE, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
-}
-template <int LOGN, int MODE, bool INV>
-void launch_row_ps(const Ctx &c, const b200::NttBatch &b, uint32_t slots, uint32_t polys, cudaStream_t st) {
-  static int cache[64] = {0};
-  constexpr int smem = b200::kRowPsSmem;
-  const uint32_t total = (1u << LOGN) / b200::kTileWords * slots * polys;
-  const unsigned grid = persistent_grid(b200::ntt_row_ps<LOGN, MODE, INV>, smem, total, c.device, cache);
-  b200::ntt_row_ps<LOGN, MODE, INV><<<grid, b200::kNttThreads, smem, st>>>(b, c.tables, slots, total);
 }
 
 // The forward row pass of a ModDown launch with its `left` operand staged in
@@ -543,7 +515,7 @@ void launch_fwd_row_epi(const Ctx &c, const b200::NttBatch &b, dim3 grid, cudaSt
 
 template <int LOGN, int MODE>
 void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
-                      bool inverse, cudaStream_t st) {
+                      bool inverse, cudaStream_t st, bool col_only) {
   const dim3 grid((1u << LOGN) / b200::kTileWords, polys, slots);
   b200::NttBatch second = b;
   second.src = b.dst;
@@ -559,26 +531,6 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     second.epi_left_stride = fin->epi_left_stride;
     second.epi_pinv = fin->epi_pinv;
   }
-  if (persistent_enabled()) {
-    require(!b.unscaled, "the persistent passes always scale by N^-1");
-    const uint32_t ns = (uint32_t)slots, np = (uint32_t)polys;
-    if (!inverse) {
-      Timed t1("ntt_fwd_col", st);
-      launch_col_ps<LOGN, MODE, false>(c, b, ns, np, st);
-      t1.done();
-      Timed t2("ntt_fwd_row", st);
-      launch_row_ps<LOGN, MODE, false>(c, second, ns, np, st);
-      t2.done();
-    } else {
-      Timed t1("ntt_inv_row", st);
-      launch_row_ps<LOGN, MODE, true>(c, b, ns, np, st);
-      t1.done();
-      Timed t2("ntt_inv_col", st);
-      launch_col_ps<LOGN, MODE, true>(c, second, ns, np, st);
-      t2.done();
-    }
-    return;
-  }
 #define NTT_LAUNCH(kernel, batch, ...)                                                        \
   do {                                                                                        \
     if (tuned("ntt_minb_" #kernel) == 3)                                                      \
@@ -593,6 +545,7 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
     else
       NTT_LAUNCH(fwd_col, b, false);
     t1.done();
+    if (col_only) return;  // the fused row pass + key multiplication finishes the transform
     Timed t2("ntt_fwd_row", st);
     if (tuned("ntt_stage_tw_fwd_row"))
       NTT_LAUNCH(fwd_row, second, true, false);
@@ -633,13 +586,13 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
 
 template <int MODE>
 void launch_ntt_chunk(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
-                      bool inverse, cudaStream_t st) {
+                      bool inverse, cudaStream_t st, bool col_only) {
   switch (c.logn) {
-    case 12: launch_ntt_2pass<12, MODE>(c, b, fin, slots, polys, inverse, st); break;
-    case 13: launch_ntt_2pass<13, MODE>(c, b, fin, slots, polys, inverse, st); break;
-    case 14: launch_ntt_2pass<14, MODE>(c, b, fin, slots, polys, inverse, st); break;
-    case 15: launch_ntt_2pass<15, MODE>(c, b, fin, slots, polys, inverse, st); break;
-    case 16: launch_ntt_2pass<16, MODE>(c, b, fin, slots, polys, inverse, st); break;
+    case 12: launch_ntt_2pass<12, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
+    case 13: launch_ntt_2pass<13, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
+    case 14: launch_ntt_2pass<14, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
+    case 15: launch_ntt_2pass<15, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
+    case 16: launch_ntt_2pass<16, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
     default: throw ContractError("unsupported ring dimension");
   }
 }
@@ -654,10 +607,15 @@ dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
 // (forward only) redirects the final pass: split destination and/or the ModDown
 // epilogue (left - x) * P^-1; small transforms run it as a separate kernel.
 // src_list (device array, one entry per polynomial) replaces src / src_stride.
+// col_only (two-pass forward transforms, mode 2): run the column pass alone;
+// the fused row pass + key multiplication (ntt_fwd_row_mac) finishes it.
 void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots_in, size_t polys,
              u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr,
-             const u64 *const *src_list = nullptr, bool unscaled = false, bool lazy_out = false) {
+             const u64 *const *src_list = nullptr, bool unscaled = false, bool lazy_out = false,
+             bool col_only = false) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
+  require(!col_only || (!inverse && !fin && c.logn >= 12 && c.mode == 2),
+          "a column pass alone is a two-pass mode-2 forward transform");
   require(!fin || !inverse, "final-pass redirection is forward only");
   require(!unscaled || (inverse && c.logn >= 12), "unscaled transforms are two-pass inverses only");
   require(!lazy_out || (!inverse && !fin && c.logn >= 12), "lazy outputs are two-pass forward transforms only");
@@ -713,11 +671,11 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
         t.done();
       }
     } else if (c.mode == 2) {
-      launch_ntt_chunk<2>(c, b, fin, (int)count, (int)polys, inverse, st);
+      launch_ntt_chunk<2>(c, b, fin, (int)count, (int)polys, inverse, st, col_only);
     } else if (c.mode == 1) {
-      launch_ntt_chunk<1>(c, b, fin, (int)count, (int)polys, inverse, st);
+      launch_ntt_chunk<1>(c, b, fin, (int)count, (int)polys, inverse, st, false);
     } else {
-      launch_ntt_chunk<0>(c, b, fin, (int)count, (int)polys, inverse, st);
+      launch_ntt_chunk<0>(c, b, fin, (int)count, (int)polys, inverse, st, false);
     }
   }
 }
@@ -909,8 +867,11 @@ void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst
 // (stride beta*T*n). copy_own = false leaves each digit's own towers unwritten
 // (the fused MAC reads them from the input).
 // src_list (device array, one input per polynomial) replaces the strided src.
+// col_only: the digits' forward transforms stop after their column pass (for
+// the fused row pass + key multiplication).
 void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carver &ws, bool copy_own,
-               cudaStream_t st, const u64 *const *src_list = nullptr, bool lazy_out = false) {
+               cudaStream_t st, const u64 *const *src_list = nullptr, bool lazy_out = false,
+               bool col_only = false) {
   const size_t n = c.n, K = c.k, T = L + K;
   const size_t beta = 1 + (L - 1) / c.alpha;
   const u64 dstride = beta * T * n;
@@ -939,7 +900,8 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
     const auto &plan = c.conv_plan(range_ids(first, first + count), tgt, unscaled);
     run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st, true);
   }
-  run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st, nullptr, nullptr, false, lazy_out);
+  run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st, nullptr, nullptr, false, lazy_out && !col_only,
+          col_only);
 }
 
 // MAC of `polys` requests: out_b/out_a of request z at out + z * out_stride;
@@ -967,24 +929,22 @@ struct MacRotation {
   uint32_t g = 1;
 };
 
-void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride,
-            const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
-            const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a, bool full_key_rows,
-            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr, bool lazy_digits = false,
-            const MacRotation &rot = {}) {
-  const size_t n = c.n, T = L + c.k;
-  const size_t beta = digits.size();
+// MAC launch arguments: `beta` digits (digit pointers optional: the fused row
+// pass reads its digits from its own arguments), keys, outputs and rotation.
+b200::MacArgs mac_args(Ctx &c, size_t L, size_t beta, u64 *out_b, u64 *out_a, u64 out_stride,
+                       const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
+                       const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a,
+                       bool full_key_rows, bool accumulate, const b200::ReqDesc *req, const MacRotation &rot) {
+  const size_t n = c.n;
   require(beta >= 1 && beta <= (size_t)b200::kMaxDigits &&
               (req || (key_b.size() == beta && key_a.size() == beta)),
           "MAC digit count out of range");
-  require(!rot.on || (mac_fuses_rotation(c, L) && beta == 1 + (L - 1) / c.alpha && !accumulate),
-          "rotation fused into the MAC needs its two-coefficient form and no accumulation");
   require(req || !rot.on || ((rot.g & 1) && rot.g < 2 * c.n), "invalid negacyclic automorphism index");
   b200::MacArgs a{};
   a.out_b = out_b;
   a.out_a = out_a;
   for (size_t d = 0; d < beta; ++d) {
-    a.digit[d] = digits[d];
+    if (d < digits.size()) a.digit[d] = digits[d];
     if (!req) {
       a.key_b[d] = key_b[d];
       a.key_a[d] = key_a[d];
@@ -1010,6 +970,20 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
     a.g = rot.g;
     a.plan = c.down_plan(L);
   }
+  return a;
+}
+
+void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stride,
+            const std::vector<const u64 *> &digits, u64 digit_poly_stride, const u64 *input,
+            const std::vector<const u64 *> &key_b, const std::vector<const u64 *> &key_a, bool full_key_rows,
+            bool accumulate, cudaStream_t st, const b200::ReqDesc *req = nullptr, bool lazy_digits = false,
+            const MacRotation &rot = {}) {
+  const size_t n = c.n, T = L + c.k;
+  const size_t beta = digits.size();
+  require(!rot.on || (mac_fuses_rotation(c, L) && beta == 1 + (L - 1) / c.alpha && !accumulate),
+          "rotation fused into the MAC needs its two-coefficient form and no accumulation");
+  const b200::MacArgs a = mac_args(c, L, beta, out_b, out_a, out_stride, digits, digit_poly_stride, input, key_b,
+                                   key_a, full_key_rows, accumulate, req, rot);
   u64 max_q = 0;
   for (auto q : c.mod) max_q = std::max(max_q, q);
   // Lazy digits lie in [0, 8q).
@@ -1069,6 +1043,41 @@ std::vector<const u64 *> key_digits(const Ctx &c, const u64 *key, size_t beta) {
   return v;
 }
 
+// Whether a key switch at level L runs its digits' forward row pass fused with
+// the key multiplication (ntt_fwd_row_mac): every modulus below 2^61, a
+// two-pass ring size, and at most row_mac_max_beta digits.
+bool row_mac_applies(const Ctx &c, size_t L) {
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  return tuned("row_mac") != 0 && c.mode == 2 && c.logn >= 12 &&
+         beta <= (size_t)std::min<int64_t>(tuned("row_mac_max_beta"), b200::kRowMacMaxBeta);
+}
+
+// The fused row pass + key multiplication over `inputs` distinct inputs whose
+// digits have been through their forward column pass (digits + u * beta*T*N).
+// Strided mode (req == nullptr): request u is input u, with the shared
+// full-context key and, with rot.on, c0 + u * rot.c0_stride. Request-table
+// mode: input u serves requests [first, first + count) of `groups`.
+void do_row_mac(Ctx &c, size_t L, size_t inputs, u64 *out_b, u64 *out_a, u64 out_stride, const u64 *digits,
+                const u64 *input, const u64 *key_b, const u64 *key_a, const b200::ReqDesc *req, const u64 *groups,
+                const MacRotation &rot, cudaStream_t st) {
+  const size_t n = c.n, T = L + c.k, beta = 1 + (L - 1) / c.alpha;
+  require(inputs >= 1 && inputs <= 65535, "request batch out of range");
+  std::vector<const u64 *> kb, ka;
+  if (!req) {
+    kb = key_digits(c, key_b, beta);
+    ka = key_digits(c, key_a, beta);
+  }
+  b200::RowMacArgs a{};
+  a.mac = mac_args(c, L, beta, out_b, out_a, out_stride, {}, beta * T * n, input, kb, ka, true, false, req, rot);
+  a.digits = digits;
+  a.digit_stride = beta * T * n;
+  a.groups = groups;
+  a.towers = (int)T;
+  Timed t("row_mac", st);
+  CUDA_CHECK(b200::row_mac_launch(a, c.tables, c.logn, (int)beta, rot.on, (unsigned)inputs, (unsigned)T, st));
+  t.done();
+}
+
 void do_rotate(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,
                u64 stride, const u64 *c0, u64 c0_stride, uint32_t g, cudaStream_t st,
                const b200::ReqDesc *req = nullptr) {
@@ -1102,9 +1111,16 @@ void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const 
   u64 *digits = ws.take(batch * beta * T * n);
   u64 *acc = ws.take(2 * batch * T * n);  // [batch][b|a][T][N]
   u64 *rot = ws.take(2 * batch * T * n);
+  if (c0) require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
+  if (row_mac_applies(c, L)) {
+    do_digits(c, L, batch, digits, src, ws, false, st, nullptr, true, true);
+    do_row_mac(c, L, batch, acc, acc + T * n, 2 * T * n, digits, src, key_b, key_a, nullptr, nullptr,
+               MacRotation{c0 != nullptr, c0, L * n, g}, st);
+    do_mod_down(c, L, 2 * batch, out_b, out_a, L * n, acc, T * n, ws, st);
+    return;
+  }
   const bool lazy = digits_lazy(c, beta);
   const bool fused = c0 && mac_fuses_rotation(c, L);
-  if (c0) require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
   do_digits(c, L, batch, digits, src, ws, false, st, nullptr, lazy);
   std::vector<const u64 *> dptr;
   for (size_t d = 0; d < beta; ++d) dptr.push_back(digits + d * T * n);
@@ -1144,8 +1160,21 @@ std::vector<Chunk> plan_chunks(const ntt_b200_ks_request *reqs, size_t count) {
   std::vector<Chunk> out;
   for (size_t L : levels) {
     Chunk cur;
+    // Requests that share an input are made adjacent (stable by digit slot),
+    // so the fused row pass finds each input's requests as one range.
     auto flush = [&] {
-      if (!cur.idx.empty()) out.push_back(std::move(cur));
+      if (!cur.idx.empty()) {
+        std::vector<size_t> order(cur.idx.size());
+        for (size_t j = 0; j < order.size(); ++j) order[j] = j;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t b) { return cur.dslot[a] < cur.dslot[b]; });
+        Chunk sorted = cur;
+        for (size_t j = 0; j < order.size(); ++j) {
+          sorted.idx[j] = cur.idx[order[j]];
+          sorted.dslot[j] = cur.dslot[order[j]];
+        }
+        out.push_back(std::move(sorted));
+      }
       cur = Chunk{};
     };
     for (size_t i = 0; i < count; ++i) {
@@ -1166,14 +1195,16 @@ std::vector<Chunk> plan_chunks(const ntt_b200_ks_request *reqs, size_t count) {
   return out;
 }
 
-// Words of a chunk's device table: ReqDesc[r] | usrc[u] | dst_list[2r] | add_list[2r].
-size_t table_words(size_t r, size_t u) { return 6 * r + u + 4 * r; }
+// Words of a chunk's device table: ReqDesc[r] | usrc[u] | dst_list[2r] |
+// add_list[2r] | groups[u] (input u's requests: first | count << 32).
+size_t table_words(size_t r, size_t u) { return 6 * r + u + 4 * r + u; }
 
 size_t chunk_bytes(const Ctx &c, const Chunk &ch) {
   const size_t n = c.n, L = ch.level, K = c.k, T = L + K, r = ch.idx.size(), u = ch.usrc.size();
   const size_t beta = 1 + (L - 1) / c.alpha;
+  const bool rot_pass = ch.rotate && !row_mac_applies(c, L) && !mac_fuses_rotation(c, L);
   return aligned_bytes(table_words(r, u)) + aligned_bytes(u * beta * T * n) + aligned_bytes(u * L * n) +
-         aligned_bytes(2 * r * T * n) + (ch.rotate && !mac_fuses_rotation(c, L) ? aligned_bytes(2 * r * T * n) : 0) +
+         aligned_bytes(2 * r * T * n) + (rot_pass ? aligned_bytes(2 * r * T * n) : 0) +
          aligned_bytes(2 * r * K * n) + aligned_bytes(2 * r * L * n);
 }
 
@@ -1219,14 +1250,27 @@ void run_chunk(Ctx &c, const ntt_b200_ks_request *reqs, const Chunk &ch, Carver 
     words.push_back(as_word(reqs[ch.idx[j]].add_b));
     words.push_back(as_word(reqs[ch.idx[j]].add_a));
   }
+  for (size_t v = 0, j = 0; v < u; ++v) {  // requests are sorted by digit slot
+    const size_t first = j;
+    while (j < r && ch.dslot[j] == v) ++j;
+    words.push_back((u64)first | ((u64)(j - first) << 32));
+  }
   put_table(words, table, st);
   const auto *desc = reinterpret_cast<const b200::ReqDesc *>(table);
   const auto *usrc = reinterpret_cast<const u64 *const *>(table + 6 * r);
   auto *dst_list = reinterpret_cast<u64 *const *>(table + 6 * r + u);
   const auto *add_list = reinterpret_cast<const u64 *const *>(table + 6 * r + u + 2 * r);
+  const u64 *groups = table + 6 * r + u + 4 * r;
 
   u64 *digits = ws.take(u * beta * T * n);
   u64 *acc = ws.take(2 * r * T * n);  // [request][b|a][T][N]
+  if (row_mac_applies(c, L)) {
+    do_digits(c, L, u, digits, nullptr, ws, false, st, usrc, true, true);
+    do_row_mac(c, L, u, acc, acc + T * n, 2 * T * n, digits, nullptr, nullptr, nullptr, desc, groups,
+               MacRotation{ch.rotate}, st);
+    do_mod_down(c, L, 2 * r, nullptr, nullptr, 0, acc, T * n, ws, st, dst_list, ch.add ? add_list : nullptr);
+    return;
+  }
   const bool fused = ch.rotate && mac_fuses_rotation(c, L);
   u64 *rot = ch.rotate && !fused ? ws.take(2 * r * T * n) : nullptr;
   const bool lazy = digits_lazy(c, beta);
@@ -1523,6 +1567,7 @@ int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const
     CUDA_CHECK(cudaMemcpy(c->d_fwd, fwd.data(), T * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
     CUDA_CHECK(cudaMemcpy(c->d_inv, inv.data(), T * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
     c->tables = b200::DeviceTables{c->d_tc, c->d_fwd, c->d_inv, c->logn};
+    CUDA_CHECK(b200::row_mac_prepare(device));
     c->table_bytes = T * sizeof(b200::TowerConsts) + 2 * T * n * sizeof(ulonglong2);
     *out = c.release();
   });

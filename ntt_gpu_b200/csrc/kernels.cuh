@@ -427,7 +427,7 @@ struct CorrectArgs {
   u64 poly_stride_dst, poly_stride_left, poly_stride_right;
   int towers, logn;
 };
-__global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
+static __global__ void __launch_bounds__(kEwThreads) correct_kernel(CorrectArgs a) {
   const u64 n = u64(1) << a.logn;
   const u64 i = u64(blockIdx.x) * blockDim.x + threadIdx.x;
   const int t = blockIdx.y;
@@ -728,7 +728,7 @@ struct RotateArgs {
   int level, m, logn;
   uint32_t g;
 };
-__global__ void __launch_bounds__(kEwThreads) rotate_kernel(RotateArgs a) {
+static __global__ void __launch_bounds__(kEwThreads) rotate_kernel(RotateArgs a) {
   const u64 n = u64(1) << a.logn;
   const u64 k = u64(blockIdx.x) * blockDim.x + threadIdx.x;
   const int t = blockIdx.y;
@@ -774,7 +774,7 @@ struct PointwiseArgs {
   uint16_t id[kMaxTowers];
   int towers, logn;
 };
-__global__ void __launch_bounds__(kEwThreads) pointwise_kernel(PointwiseArgs a) {
+static __global__ void __launch_bounds__(kEwThreads) pointwise_kernel(PointwiseArgs a) {
   const u64 n = u64(1) << a.logn;
   const u64 i = u64(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;

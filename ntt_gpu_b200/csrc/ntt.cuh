@@ -708,7 +708,7 @@ __global__ void __launch_bounds__(kNttThreads) ntt_small(NttBatch b, DeviceTable
 // values stay in [0, 8q); they are folded into one word that is stored only
 // if it equals a fixed constant, so the work cannot be dropped. This measures
 // the multiply-pipe ceiling that bounds the NTT passes on the running GPU.
-__global__ void __launch_bounds__(kNttThreads, 4)
+static __global__ void __launch_bounds__(kNttThreads, 4)
     butterfly_rate_kernel(u64 *sink, u64 q, Shoup w0, Shoup w1, Shoup w2, Shoup w3, int rounds) {
   const u64 q2 = 2 * q;
   u64 x[16];

@@ -1,0 +1,218 @@
+// Forward row pass of the Hybrid digits fused with the key multiplication.
+//
+// The key switch's digits (Session::hybrid_digits, src/resident.cpp:458-491)
+// are used once, by the MAC (Session::hybrid_accumulate, src/resident.cpp:
+// 530-570, hybrid_mac_value of include/ntt/resident_conversion.hpp:50-54).
+// Here one CTA takes one QP tower t, one block of 2 * WARPS rows (256 words
+// each) and one distinct input. It runs the forward NTT's row pass (the last
+// 8 stages) of every digit that has to be transformed at that tower, keeps the
+// transformed rows in shared memory, and then forms, for every request that
+// shares the input,
+//   Z_b[t] = sum_d D_d[t] * KB_d[row(t)],  Z_a[t] = sum_d D_d[t] * KA_d[row(t)]
+// with exact 128-bit sums and one reduction per output; the digit a Q tower
+// belongs to is read from the input itself (it is the input's own tower). The
+// digits never reach HBM: the separate MAC pass, and its re-read of every
+// digit tower, is gone. With ROT, the rotation of the extended result happens
+// in the same stores (P * c0 added on b's Q towers, slot i stored at the slot
+// the automorphism moves it to; resident_hybrid_rotate_kernel of
+// src/cuda/resident_adapter.inc:44-59).
+//
+// Layout: each warp owns two rows through both register phases of every
+// digit's row pass and through the MAC, so the CTA never synchronises; its
+// dynamic shared memory holds one padded region of 2 * WARPS rows per digit it
+// transforms. The Q towers (beta - 1 digits: their own digit is the input) and
+// the P towers (beta digits) run as two launches with their own region counts,
+// so the common Q towers fit three CTAs per SM at beta = 3.
+// Arithmetic: every modulus below 2^61 (butterfly mode 2). Digits stay in the
+// butterflies' lazy range [0, 8q); keys and the input are canonical, so with
+// at most 4 digits the sums stay below 4 * 8q * q < 2^127 and the
+// approximate-quotient reduction (reduce128_approx) applies.
+#pragma once
+#include <cstdint>
+
+#include "arith.cuh"
+#include "kernels.cuh"
+#include "ntt.cuh"
+#include "tables.cuh"
+
+namespace b200 {
+
+struct RowMacArgs {
+  MacArgs mac;            // outputs, keys, input, request table, rotation (see mac2_kernel)
+  const u64 *digits;      // digit d of tower t, distinct input u: digits + u * digit_stride + (d * towers + t) * n
+  u64 digit_stride;
+  const u64 *groups;      // request-table mode: per distinct input, first request | count << 32
+  int towers;             // L + K
+};
+
+// Shared memory of one launch: Q towers transform beta - 1 digits (their own
+// digit is the input), P towers all beta. Regions of 2 * WARPS padded rows.
+template <int WARPS>
+constexpr int row_mac_smem_bytes(int regions) {
+  return regions * 2 * WARPS * kRowPad * int(sizeof(u64));
+}
+
+// 8-byte global -> shared copy that completes asynchronously (cp.async groups).
+__device__ __forceinline__ void rm_copy8(u64 *smem, const u64 *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+
+// PT: the launch covers the P towers (tower t = L + blockIdx.z), else the Q
+// towers (t = blockIdx.z). The digits a CTA transforms run in order through
+// shared-memory regions 0, 1, ...; the rows of the next one are copied into
+// its region (cp.async) while the current one's butterflies run.
+template <int LOGN, int BETA, int WARPS, bool ROT, bool PT>
+__global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, DeviceTables T) {
+  constexpr int LR = LOGN - 8;
+  constexpr u64 N = u64(1) << LOGN;
+  constexpr int kRows = 2 * WARPS;  // rows per CTA
+  extern __shared__ __align__(16) u64 rm_digits[];  // [regions][kRows][kRowPad]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int h = lane >> 4, u = lane & 15;
+  const int L = a.mac.level;
+  const int t = PT ? L + int(blockIdx.z) : int(blockIdx.z);
+  const int gid = PT ? a.mac.m + int(blockIdx.z) : t;  // global tower id (key_indices, backend_contract.hpp:112-119)
+  const TowerConsts *tc = T.tc + gid;
+  const u64 q = tc->q, q2 = tc->q2;
+  const ulonglong2 *tw = T.fwd + u64(gid) * N;
+  const int wrow = blockIdx.x * kRows + 2 * warp;  // the warp's first row
+  const int row = wrow + h;
+  const u64 input = blockIdx.y;
+  const int own = PT ? -1 : t / a.mac.alpha;
+  constexpr int kMaxRegions = PT ? BETA : BETA - 1;
+  // Digit of region i, and the source rows of a digit.
+  auto digit_of = [&](int i) { return PT ? i : (i < own ? i : i + 1); };
+  // The copy's addresses are rebuilt from a laundered lane index each time, so
+  // none of them stays live across the butterflies of the digit in flight.
+  auto stage_rows = [&](int i) {
+    uint32_t ln = lane;
+    asm volatile("" : "+r"(ln));
+    const u64 *src = a.digits + input * a.digit_stride + (u64(digit_of(i)) * a.towers + t) * N + u64(wrow) * 256;
+    u64 *dst = rm_digits + (i * kRows + 2 * warp) * kRowPad;
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+      const int j = int(ln) + 32 * k, rr = j >> 8, c = j & 255;
+      rm_copy8(dst + rr * kRowPad + pad_col(c), src + rr * 256 + c);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if constexpr (kMaxRegions > 0) stage_rows(0);
+
+  // Row passes (stages logR .. logN-1) of the digits this tower transforms.
+#pragma unroll 1
+  for (int i = 0; i < kMaxRegions; ++i) {
+    if (i + 1 < kMaxRegions) {
+      stage_rows(i + 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncwarp();
+    u64 *my = rm_digits + (i * kRows + 2 * warp + h) * kRowPad;
+    u64 x[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp) {
+      const int s = LR + sp, dd = 8 >> sp;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & dd) continue;
+        const Shoup w = tw_load(tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
+        ct_butterfly<2>(x[e], x[e + dd], w.w, w.wq, q, q2);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
+#pragma unroll
+    for (int sp = 4; sp < 8; ++sp) {
+      const int s = LR + sp, dd = 1 << (7 - sp);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & dd) continue;
+        const Shoup w = tw_load(tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
+        ct_butterfly<2>(x[e], x[e + dd], w.w, w.wq, q, q2);
+      }
+    }
+    // Each thread overwrites exactly the words it has just read: no barrier.
+#pragma unroll
+    for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
+  }
+  __syncwarp();
+
+  // Key multiplication over the warp's two rows: 2 adjacent coefficients per
+  // lane and step, 16-byte loads of the input's own tower and of the keys.
+  const Reducer red = tc->red;
+  u64 first = input, count = 1;
+  if (a.groups) {
+    const u64 gw = a.groups[input];
+    first = gw & 0xFFFFFFFFu;
+    count = gw >> 32;
+  }
+  for (u64 z = first; z < first + count; ++z) {
+    const MacBases mb = mac_bases(a.mac, z);
+    const u64 *kb[BETA], *ka[BETA];
+#pragma unroll
+    for (int d = 0; d < BETA; ++d) {
+      kb[d] = (a.mac.req ? mb.kb + d * a.mac.key_digit_stride : a.mac.key_b[d]) + u64(gid) * N;
+      ka[d] = (a.mac.req ? mb.ka + d * a.mac.key_digit_stride : a.mac.key_a[d]) + u64(gid) * N;
+    }
+    const u64 obase = z * a.mac.poly_stride_out + u64(t) * N;
+    const uint32_t gi = ROT ? inverse_mod_pow2(mb.g) : 1u;
+    Shoup pm{0, 0};
+    if (ROT && mb.c0 && !PT) pm = a.mac.plan->p_mod[t];
+#pragma unroll 2
+    for (int it = 0; it < 8; ++it) {
+      const int j = lane + 32 * it;
+      const int rr = j >> 7, c = (j & 127) * 2;
+      const u64 i = u64(wrow + rr) * 256 + c;
+      Acc128 b0{}, b1{}, a0{}, a1{};
+#pragma unroll
+      for (int d = 0; d < BETA; ++d) {
+        ulonglong2 x;
+        if (!PT && d == own) {
+          x = *reinterpret_cast<const ulonglong2 *>(mb.input + u64(t) * N + i);
+        } else {
+          const int region = PT ? d : (d < own ? d : d - 1);
+          const u64 *sd = rm_digits + (region * kRows + 2 * warp + rr) * kRowPad + pad_col(c);
+          x = make_ulonglong2(sd[0], sd[1]);
+        }
+        const ulonglong2 vb = *reinterpret_cast<const ulonglong2 *>(kb[d] + i);
+        const ulonglong2 va = *reinterpret_cast<const ulonglong2 *>(ka[d] + i);
+        acc_mad(b0, x.x, vb.x);
+        acc_mad(b1, x.y, vb.y);
+        acc_mad(a0, x.x, va.x);
+        acc_mad(a1, x.y, va.y);
+      }
+      ulonglong2 rb, ra;
+      rb.x = reduce128_approx((u64)b0.v, (u64)(b0.v >> 64), red);
+      rb.y = reduce128_approx((u64)b1.v, (u64)(b1.v >> 64), red);
+      ra.x = reduce128_approx((u64)a0.v, (u64)(a0.v >> 64), red);
+      ra.y = reduce128_approx((u64)a1.v, (u64)(a1.v >> 64), red);
+      if constexpr (ROT) {
+        if (!PT && mb.c0) {  // rotated_b_value: b + P * c0 on the Q towers
+          const ulonglong2 cc = *reinterpret_cast<const ulonglong2 *>(mb.c0 + u64(t) * N + i);
+          rb.x = add_mod(rb.x, shoup_canon(cc.x, pm.w, pm.wq, red.m), red.m);
+          rb.y = add_mod(rb.y, shoup_canon(cc.y, pm.w, pm.wq, red.m), red.m);
+        }
+        const u64 d0 = obase + automorphism_source((uint32_t)i, LOGN, gi);
+        const u64 d1 = obase + automorphism_source((uint32_t)i + 1, LOGN, gi);
+        a.mac.out_b[d0] = rb.x;
+        a.mac.out_b[d1] = rb.y;
+        a.mac.out_a[d0] = ra.x;
+        a.mac.out_a[d1] = ra.y;
+      } else {
+        *reinterpret_cast<ulonglong2 *>(a.mac.out_b + obase + i) = rb;
+        *reinterpret_cast<ulonglong2 *>(a.mac.out_a + obase + i) = ra;
+      }
+    }
+  }
+}
+
+}  // namespace b200

@@ -1,0 +1,88 @@
+"""The key multiplication fused into the digits' forward row pass
+(ntt_fwd_row_mac) against the separate row pass + MAC pipeline.
+
+Both forms must give the same key switches bit for bit: strided batches with
+a shared key, with and without rotation, and request lists that mix keys,
+rotations, relinearization addends and inputs shared by several requests
+(hoisted digits, where one CTA serves every request of its input). Digit
+counts 1 to 4 are covered (row_mac_max_beta selects per count)."""
+import numpy as np
+import pytest
+
+import ntt_gpu_b200 as nb
+from oracle.oracle import synthetic_context
+from test_gpu_requests import Case, _keys
+
+pytestmark = pytest.mark.gpu
+
+
+def _sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+def _batch(g, ctx, level, batch, xs, kb, ka, c0=None, auto=0):
+    ob, oa = nb.empty((batch, level, ctx.n)), nb.empty((batch, level, ctx.n))
+    g.keyswitch_batch(level, batch, ob, oa, xs, kb, ka, g.workspace(nb.OP_KEYSWITCH, level, batch), c0=c0,
+                      automorphism=auto)
+    _sync()
+    return nb.to_host(ob), nb.to_host(oa)
+
+
+@pytest.mark.parametrize("n,m,k,dnum,levels", [(65536, 24, 8, 3, (24, 16, 8)), (16384, 32, 8, 4, (32, 25, 9, 3)),
+                                               (4096, 12, 6, 2, (12, 6))])
+def test_fused_batch_equals_separate_passes(lib, orc, n, m, k, dnum, levels):
+    ctx = synthetic_context(orc, n, m, k, dnum)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka, dkb, dka = _keys(orc, ctx, 41)
+    for level in levels:
+        batch = 3
+        xs = nb.to_device(np.stack([orc.lcg(n, ctx.q[:level], 60 + i) for i in range(batch)]))
+        c0 = nb.to_device(np.stack([orc.lcg(n, ctx.q[:level], 70 + i) for i in range(batch)]))
+        got = {}
+        for fused in (1, 0):
+            nb.tuning_set("row_mac", fused)
+            try:
+                got[fused] = (_batch(g, ctx, level, batch, xs, dkb, dka), _batch(g, ctx, level, batch, xs, dkb, dka,
+                                                                                    c0, 25))
+            finally:
+                nb.tuning_set("row_mac", 1)
+        for a, b in zip(got[1], got[0]):
+            np.testing.assert_array_equal(a[0], b[0], err_msg=f"L={level}")
+            np.testing.assert_array_equal(a[1], b[1], err_msg=f"L={level}")
+        # one request of each checked against the oracle
+        x0 = orc.lcg(n, ctx.q[:level], 60)
+        wb, wa = orc.keyswitch(ctx, level, x0, kb, ka, orc.lcg(n, ctx.q[:level], 70), 25)
+        np.testing.assert_array_equal(got[1][1][0][0], wb)
+        np.testing.assert_array_equal(got[1][1][1][0], wa)
+    assert g.device_errors() == 0
+    g.close()
+
+
+def test_fused_request_list_with_shared_inputs(lib, orc):
+    """Hoisted rotations (several keys and automorphisms over one input) next
+    to distinct inputs and relinearizations, at two levels: equal to the
+    oracle with the fused row pass."""
+    ctx = synthetic_context(orc, 8192, 9, 3, 3)
+    g = nb.Context.from_oracle(ctx)
+    keysets = [_keys(orc, ctx, 300 + 7 * i) for i in range(3)]
+    cases = []
+    for level in (9, 5):
+        base = Case(orc, ctx, level, 1000 + level, keysets[0], "rotate", 5)
+        cases.append(base)
+        for i, auto in enumerate((25, 2 * ctx.n - 1, 125)):
+            cases.append(Case(orc, ctx, level, 1100 + 10 * level + i, keysets[(i + 1) % 3], "rotate", auto,
+                              share=base))
+        cases.append(Case(orc, ctx, level, 1200 + level, keysets[1], "switch", share=base))
+        cases.append(Case(orc, ctx, level, 1300 + level, keysets[2], "relin"))
+        cases.append(Case(orc, ctx, level, 1400 + level, keysets[0], "switch"))
+    # interleave so requests of one input are not adjacent in the call
+    order = cases[::2] + cases[1::2]
+    reqs = [c.request() for c in order]
+    g.keyswitch_requests(reqs, g.requests_workspace(reqs))
+    _sync()
+    for c in order:
+        wb, wa = c.expected(orc, ctx)
+        np.testing.assert_array_equal(nb.to_host(c.out_b), wb, err_msg=f"{c.kind} L={c.level}")
+        np.testing.assert_array_equal(nb.to_host(c.out_a), wa, err_msg=f"{c.kind} L={c.level}")
+    g.close()
