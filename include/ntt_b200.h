@@ -378,8 +378,10 @@ const char *ntt_b200_tuning_name(size_t index);
  * larger requests are refused with a contract error. The caller still passes
  * the input and output. The level's tables must exist already
  * (ntt_b200_context_prepare); this call allocates nothing. Its first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture. All calls share the one array and
+ * device looks up the array's device address (cudaGetSymbolAddress) and keeps
+ * it for the life of the process, so make that first call before any stream
+ * capture; the address belongs to the device's primary context, so the entry
+ * point must not be used after cudaDeviceReset on that device. All calls share the one array and
  * it keeps the previous call's contents (nothing in it needs to start at zero):
  * calls that overlap on the GPU - on different streams, or on one device from
  * different contexts - race on it. This entry point has no counterpart in the
@@ -387,6 +389,63 @@ const char *ntt_b200_tuning_name(size_t index);
 size_t ntt_b200_mod_down_static_max_bytes(void);
 int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, const uint64_t *src,
                              void *stream);
+
+/* Host-buffer transforms: the reference's CudaNttTransform public calls
+ * forward / inverse / pointwise_multiply / multiply (include/ntt/cuda_ntt.hpp:59-66;
+ * src/cuda/ntt_kernels.cu:423-488). `values` (and `right`) are limb-major HOST
+ * arrays of `towers` towers of N words, tower i using the tables of global tower
+ * tower_ids[i]:
+ *   FORWARD / INVERSE: values transformed in place (natural coefficients <->
+ *     bit-reversed evaluations, as ntt_b200_ntt);
+ *   POINTWISE: values *= right (both evaluation form);
+ *   MULTIPLY: values = the ring product of values and right mod x^N + 1
+ *     (coefficient form in and out).
+ * Every residue is checked against its tower's modulus on the host before
+ * anything is enqueued (the reference's validate_values; a contract error
+ * otherwise). The call is synchronous, like the reference's: it returns once
+ * the results are back in host memory. The towers move in chunks of 4 through
+ * two device staging slots in `workspace` (ntt_b200_host_transform_workspace
+ * bytes), on the context's copy streams, so host->device copies, transforms
+ * and device->host copies of different chunks overlap (with pinned host memory;
+ * pageable memory works, with less overlap). */
+#define NTT_B200_HOST_FORWARD 0
+#define NTT_B200_HOST_INVERSE 1
+#define NTT_B200_HOST_POINTWISE 2
+#define NTT_B200_HOST_MULTIPLY 3
+int ntt_b200_host_transform_workspace(ntt_b200_context ctx, int op, size_t *bytes);
+int ntt_b200_host_transform(ntt_b200_context ctx, int op, uint64_t *values, const uint64_t *right,
+                            const uint32_t *tower_ids, size_t towers, void *workspace,
+                            size_t workspace_bytes, void *stream);
+
+/* Device arithmetic probes: the reference's shoup_kernel / barrett_kernel
+ * checks of its device arithmetic against host 128-bit arithmetic
+ * (tests/basis_cuda.cu:49-65). `count` queries of 5 words each (device array),
+ * one result word each (device array):
+ *   op 0: (x, w, floor(w 2^64 / q), q, -)  -> x w mod q, Shoup, canonical
+ *         (include/ntt/shoup.hpp:7-27);
+ *   op 1: (a, b, q, mu_lo, mu_hi)          -> a b mod q, Barrett with
+ *         mu = floor(2^128 / q), canonical (include/ntt/barrett.hpp:10-50);
+ *   op 2: (x, w, floor(w 2^64 / q), q, -)  -> the NTT's approximate-quotient
+ *         Shoup product, congruent to x w and in [0, 4q) for q < 2^61. */
+int ntt_b200_arith_probe(int device, int op, const uint64_t *queries, size_t count, uint64_t *out,
+                         void *stream);
+
+/* Test hooks (no counterpart in the reference's public API; its tests reach
+ * the same seams through private constructors):
+ *  - conv_wait_polls: poll limit of the tensor-core conversion's first bounded
+ *    wait (default and maximum 2^20). 0 makes that wait give up at once: the
+ *    kernel then waits (bounded, at the full limit) for its own bulk copy,
+ *    frees its tensor memory, returns, and reports the timeout through
+ *    ntt_b200_device_errors (its outputs are then invalid). Nothing hangs.
+ *  - inject_setup_failure: the next ntt_b200_context_create fails with a CUDA
+ *    error before its `operation`-th device allocation or upload (1-based; 0
+ *    turns it off) and releases everything it had set up, as the reference's
+ *    SetupResources unwinds (include/ntt/setup_resources.hpp:19-60);
+ *  - setup_operations: the allocations and uploads of the last successful
+ *    ntt_b200_context_create. */
+int ntt_b200_conv_wait_polls(int polls);
+int ntt_b200_inject_setup_failure(size_t operation);
+int ntt_b200_setup_operations(size_t *count);
 
 /* Opt-in per-kernel timing: while enabled, every launch of this library is
  * bracketed by CUDA events on its own stream. query() waits for the recorded

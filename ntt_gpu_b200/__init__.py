@@ -109,7 +109,15 @@ _SIGNATURES = {
     "ntt_b200_timing_reset": ([], _I),
     "ntt_b200_timing_query": ([ctypes.c_char_p, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double)], _I),
     "ntt_b200_butterfly_rate": ([_I, ctypes.POINTER(ctypes.c_double)], _I),
+    "ntt_b200_host_transform_workspace": ([_P, _I, ctypes.POINTER(_SZ)], _I),
+    "ntt_b200_host_transform": ([_P, _I, _P, _P, _P, _SZ, _P, _SZ, _P], _I),
+    "ntt_b200_arith_probe": ([_I, _I, _P, _SZ, _P, _P], _I),
+    "ntt_b200_conv_wait_polls": ([_I], _I),
+    "ntt_b200_inject_setup_failure": ([_SZ], _I),
+    "ntt_b200_setup_operations": ([ctypes.POINTER(_SZ)], _I),
 }
+
+HOST_FORWARD, HOST_INVERSE, HOST_POINTWISE, HOST_MULTIPLY = 0, 1, 2, 3
 
 
 class KsRequest(ctypes.Structure):
@@ -395,6 +403,29 @@ class Context:
                                                  _ptr(key_b), _ptr(key_a), hp(h_c0), automorphism, _ptr(workspace),
                                                  workspace.numel() * 8, _stream(stream)))
 
+    def host_transform_workspace(self, op):
+        import torch
+        out = _SZ()
+        _check(self._lib.ntt_b200_host_transform_workspace(self._h, int(op), ctypes.byref(out)))
+        return torch.empty(max(1, (out.value + 7) // 8), dtype=torch.int64, device=f"cuda:{self.device}")
+
+    def host_transform(self, op, values, tower_ids, workspace, right=None, stream=None):
+        """The reference's CudaNttTransform public calls on host arrays (numpy
+        uint64 or CPU int64 tensors, limb-major, contiguous), synchronous and in
+        place on `values`: HOST_FORWARD, HOST_INVERSE, HOST_POINTWISE (values *=
+        right), HOST_MULTIPLY (ring product)."""
+        def hp(a):
+            if a is None:
+                return None
+            if hasattr(a, "ctypes"):
+                assert a.dtype.itemsize == 8 and a.flags["C_CONTIGUOUS"]
+                return a.ctypes.data
+            assert not a.is_cuda and a.is_contiguous()
+            return a.data_ptr()
+        ids = _arr(tower_ids, ctypes.c_uint32)
+        _check(self._lib.ntt_b200_host_transform(self._h, int(op), hp(values), hp(right), ids, len(tower_ids),
+                                                 _ptr(workspace), workspace.numel() * 8, _stream(stream)))
+
     def keyswitch(self, level, out_b, out_a, src, key_b, key_a, workspace, c0=None, automorphism=0,
                   stream=None):
         _check(self._lib.ntt_b200_keyswitch(self._h, level, _ptr(out_b), _ptr(out_a), _ptr(src), _ptr(key_b),
@@ -520,6 +551,18 @@ class KeyCache:
 
 KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col", "ntt_small", "conv", "mac",
                   "row_mac", "rotate", "correct", "pointwise", "table")
+
+
+def arith_probe(op: int, queries, device: int = 0):
+    """Device arithmetic probe (ntt_b200_arith_probe): queries is a [count][5]
+    uint64 numpy array; returns the [count] results computed on the GPU."""
+    import numpy as np
+    import torch
+    q = to_device(np.ascontiguousarray(queries, dtype=np.uint64), device)
+    out = torch.empty((q.shape[0],), dtype=torch.int64, device=f"cuda:{device}")
+    _check(load().ntt_b200_arith_probe(device, int(op), q.data_ptr(), q.shape[0], out.data_ptr(),
+                                       torch.cuda.current_stream(device).cuda_stream))
+    return to_host(out)
 
 
 def butterfly_rate(device: int = 0) -> float:

@@ -15,9 +15,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libntt_b200.so")
-HOST = os.path.join(HERE, "host")
-HOST_LIB = os.path.join(LIB_DIR, "libntt_b200_host.so")
-CXX_FLAGS = ["-std=c++20", "-O2", "-Wall", "-Wextra", "-fPIC", "-shared"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -25,14 +22,6 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
 def sources() -> list[str]:
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)
                   if f.endswith((".cu", ".cuh", ".cpp", ".h", ".hpp")))
-
-
-def host_sources() -> list[str]:
-    out = []
-    for sub in ("src", os.path.join("include", "ntt_b200")):
-        d = os.path.join(HOST, sub)
-        out += sorted(os.path.join(d, f) for f in os.listdir(d))
-    return out
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -44,22 +33,7 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 def stale() -> bool:
     header = os.path.join(HERE, "..", "include", "ntt_b200.h")
-    return (_stale(LIB, sources() + [header, __file__]) or
-            _stale(HOST_LIB, host_sources() + [header, __file__, LIB]))
-
-
-def build_host(verbose: bool = False) -> str:
-    """C++ resident runtime (Session + B200 driver) linked against libntt_b200.so."""
-    cxx = shutil.which("g++") or "g++"
-    tmp = HOST_LIB + ".tmp"
-    srcs = [os.path.join(HOST, "src", f) for f in ("session.cpp", "b200_driver.cpp")]
-    cmd = [cxx, *CXX_FLAGS, "-I", os.path.join(HOST, "include"), "-o", tmp, *srcs,
-           "-L", LIB_DIR, "-lntt_b200", "-Wl,-rpath,$ORIGIN"]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, HOST_LIB)
-    return HOST_LIB
+    return _stale(LIB, sources() + [header, __file__])
 
 
 # Translation units of libntt_b200.so, compiled in parallel to objects under
@@ -97,5 +71,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         os.replace(tmp, LIB)
-    build_host(verbose)
     return LIB

@@ -227,4 +227,25 @@ __device__ __forceinline__ u64 reduce_out(const Acc192 &a, const Reducer &r) {
 __device__ __forceinline__ u64 mul_mod(u64 a, u64 b, const Reducer &r) {
   return reduce128(a * b, mulhi(a, b), r);
 }
+
+// ---- Barrett multiplication (include/ntt/barrett.hpp:10-50) ---------------------
+// With mu = floor(2^128 / q) (mu_lo + 2^64 mu_hi) and x = a * b < q^2 < 2^126,
+// e = floor(x * mu / 2^128) is floor(x / q) or one below it, so x - e q lies in
+// [0, 2q) and is exact in its low 64 bits; one conditional subtraction ends it.
+// Writing x = xh 2^64 + xl, x * mu / 2^128 = xh mu_hi + (xh mu_lo + xl mu_hi +
+// hi(xl mu_lo)) / 2^64 + (a fraction that cannot carry), so e is xh mu_hi plus
+// the high words of the two cross products plus the carry out of their low
+// words and hi(xl mu_lo). e < q < 2^63 fits one word, so its products wrap.
+struct Barrett {
+  u64 q, mu_lo, mu_hi;
+};
+__device__ __forceinline__ u64 barrett_mul(u64 a, u64 b, const Barrett &p) {
+  const u64 xl = a * b, xh = mulhi(a, b);
+  const u64 c1 = xh * p.mu_lo, c2 = xl * p.mu_hi;  // low words of the cross products
+  const u64 t = c1 + c2;
+  const u64 u = t + mulhi(xl, p.mu_lo);
+  const u64 carry = u64(t < c1) + u64(u < t);
+  const u64 e = xh * p.mu_hi + mulhi(xh, p.mu_lo) + mulhi(xl, p.mu_hi) + carry;
+  return csub(xl - e * p.q, p.q);
+}
 }  // namespace b200

@@ -15,6 +15,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -32,6 +33,11 @@ using u128 = unsigned __int128;
 namespace {
 thread_local std::string g_last_error;
 std::atomic<uint64_t> g_launches{0};
+// Test hooks, off by default: the poll limit of the tensor-core conversion's
+// first bounded wait, and a context-setup operation to fail (0 = none).
+std::atomic<int> g_conv_first_wait{1 << 20};
+std::atomic<size_t> g_setup_fail_at{0};
+std::atomic<size_t> g_setup_operations{0};
 
 struct ContractError : std::invalid_argument {
   using std::invalid_argument::invalid_argument;
@@ -45,8 +51,14 @@ struct CudaError : std::runtime_error {
 void require(bool ok, const char *why) {
   if (!ok) throw ContractError(why);
 }
+// A failed runtime call also leaves its (non-sticky) error as the thread's
+// last error; it is cleared here so that a later, unrelated launch check does
+// not report it again.
 void check_cuda(cudaError_t e, const char *call) {
-  if (e != cudaSuccess) throw CudaError(std::string("CUDA: ") + call + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw CudaError(std::string("CUDA: ") + call + ": " + cudaGetErrorString(e));
+  }
 }
 #define CUDA_CHECK(x) check_cuda((x), #x)
 
@@ -731,6 +743,7 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   a.logn = c.logn;
   a.kpad = p.tc_kpad;
   a.groups = p.tc_groups;
+  a.first_wait_polls = g_conv_first_wait.load(std::memory_order_relaxed);
   a.err = c.d_err;
   const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad +
                    p.s * b200::kTcThreads * (int)sizeof(u64);
@@ -1558,14 +1571,32 @@ int ntt_b200_context_create(ntt_b200_context *out, int device, uint64_t n, const
       tc[g].red = h_reducer(mq);
     }
     DeviceGuard guard(device);
+    // Every device allocation and upload of the setup is one operation; an
+    // injected failure (ntt_b200_inject_setup_failure) throws before the
+    // chosen one, and the partly built context unwinds through its destructor
+    // (the reference's SetupResources, include/ntt/setup_resources.hpp:19-60).
+    const size_t fail_at = g_setup_fail_at.exchange(0);
+    size_t ops = 0;
+    auto step = [&] {
+      if (++ops == fail_at) throw CudaError("CUDA: injected failure before setup operation " + std::to_string(ops));
+    };
+    step();
     CUDA_CHECK(cudaMalloc(&c->d_tc, T * sizeof(b200::TowerConsts)));
+    step();
     CUDA_CHECK(cudaMalloc(&c->d_err, sizeof(int)));
+    step();
     CUDA_CHECK(cudaMemset(c->d_err, 0, sizeof(int)));
+    step();
     CUDA_CHECK(cudaMalloc(&c->d_fwd, T * n * sizeof(ulonglong2)));
+    step();
     CUDA_CHECK(cudaMalloc(&c->d_inv, T * n * sizeof(ulonglong2)));
+    step();
     CUDA_CHECK(cudaMemcpy(c->d_tc, tc.data(), T * sizeof(b200::TowerConsts), cudaMemcpyHostToDevice));
+    step();
     CUDA_CHECK(cudaMemcpy(c->d_fwd, fwd.data(), T * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    step();
     CUDA_CHECK(cudaMemcpy(c->d_inv, inv.data(), T * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    g_setup_operations = ops;
     c->tables = b200::DeviceTables{c->d_tc, c->d_fwd, c->d_inv, c->logn};
     CUDA_CHECK(b200::row_mac_prepare(device));
     c->table_bytes = T * sizeof(b200::TowerConsts) + 2 * T * n * sizeof(ulonglong2);
@@ -1917,6 +1948,22 @@ int ntt_b200_keyswitch_requests(ntt_b200_context ctx, const ntt_b200_ks_request 
 }
 
 // ---- host-buffer key switch with overlapped copies ------------------------------------
+namespace {
+// Copy streams and slot events of the host-buffer pipelines (pipe_mu held).
+void ensure_copy_pipeline(Ctx &c) {
+  if (c.copy_in) return;
+  DeviceGuard guard(c.device);
+  CUDA_CHECK(cudaStreamCreateWithFlags(&c.copy_in, cudaStreamNonBlocking));
+  CUDA_CHECK(cudaStreamCreateWithFlags(&c.copy_out, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; ++i) {
+    CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_in[i], cudaEventDisableTiming));
+    CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_comp[i], cudaEventDisableTiming));
+    CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_out[i], cudaEventDisableTiming));
+  }
+  CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_start, cudaEventDisableTiming));
+}
+}  // namespace
+
 size_t host_slot_words(const Ctx &c, size_t level, size_t chunk, bool rotate) {
   return chunk * level * c.n * (rotate ? 4 : 3);  // src (+ c0) in, out_b + out_a
 }
@@ -1952,16 +1999,7 @@ int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, si
     c.conv_plan(range_ids(c.m, c.m + c.k), range_ids(0, level), intt_unscaled(c));
     c.down_plan(level);
     std::lock_guard<std::mutex> lock(c.pipe_mu);
-    if (!c.copy_in) {
-      CUDA_CHECK(cudaStreamCreateWithFlags(&c.copy_in, cudaStreamNonBlocking));
-      CUDA_CHECK(cudaStreamCreateWithFlags(&c.copy_out, cudaStreamNonBlocking));
-      for (int i = 0; i < 2; ++i) {
-        CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_in[i], cudaEventDisableTiming));
-        CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_comp[i], cudaEventDisableTiming));
-        CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_out[i], cudaEventDisableTiming));
-      }
-      CUDA_CHECK(cudaEventCreateWithFlags(&c.ev_start, cudaEventDisableTiming));
-    }
+    ensure_copy_pipeline(c);
     const cudaStream_t st = as_stream(stream);
     char *base = reinterpret_cast<char *>(workspace);
     u64 *slot[2] = {reinterpret_cast<u64 *>(base), reinterpret_cast<u64 *>(base + aligned_bytes(slot_words))};
@@ -2175,6 +2213,174 @@ int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, 
     DeviceGuard guard(c.device);
     Carver ws{reinterpret_cast<char *>(scratch), kStaticScratchWords * sizeof(uint64_t)};
     do_mod_down(c, level, 1, dst, nullptr, 0, src, 0, ws, as_stream(stream));
+  });
+}
+}  // extern "C"
+
+// ---- host-buffer transforms (the reference's CudaNttTransform public calls) ---------------
+namespace {
+constexpr size_t kHostChunkTowers = 4;  // towers per staging slot and operand
+
+size_t host_transform_slot_words(const Ctx &c, int op) {
+  return (op >= NTT_B200_HOST_POINTWISE ? 2 : 1) * kHostChunkTowers * c.n;
+}
+
+// Every residue below its tower's modulus (the reference's validate_values),
+// on the host before anything is enqueued; large inputs are split over threads.
+void validate_host_values(const Ctx &c, const u64 *v, const std::vector<uint16_t> &ids) {
+  const size_t n = c.n, towers = ids.size();
+  auto scan = [&](size_t t0, size_t t1) {
+    bool ok = true;
+    for (size_t t = t0; t < t1; ++t) {
+      const u64 q = c.mod[ids[t]];
+      const u64 *p = v + t * n;
+      u64 bad = 0;
+      for (size_t i = 0; i < n; ++i) bad |= u64(p[i] >= q);
+      ok = ok && bad == 0;
+    }
+    return ok;
+  };
+  const size_t threads = std::min<size_t>(towers, towers * n >= (size_t(1) << 20) ? 8 : 1);
+  bool ok = true;
+  if (threads <= 1) {
+    ok = scan(0, towers);
+  } else {
+    std::vector<std::thread> pool;
+    std::vector<char> part(threads, 1);
+    for (size_t w = 0; w < threads; ++w)
+      pool.emplace_back([&, w] { part[w] = scan(towers * w / threads, towers * (w + 1) / threads); });
+    for (auto &th : pool) th.join();
+    for (char r : part) ok = ok && r;
+  }
+  require(ok, "host values must be canonical residues of their towers");
+}
+
+void launch_pointwise(const Ctx &c, u64 *dst, const u64 *left, const u64 *right, const std::vector<Slot> &slots,
+                      cudaStream_t st) {
+  b200::PointwiseArgs a{};
+  a.dst = dst;
+  a.left = left;
+  a.right = right;
+  a.tc = c.d_tc;
+  a.poly_stride = 0;
+  for (size_t i = 0; i < slots.size(); ++i) a.id[i] = slots[i].id;
+  a.towers = (int)slots.size();
+  a.logn = c.logn;
+  Timed t("pointwise", st);
+  b200::pointwise_kernel<<<ew_grid(c, slots.size(), 1), b200::kEwThreads, 0, st>>>(a);
+  t.done();
+}
+}  // namespace
+
+extern "C" {
+int ntt_b200_host_transform_workspace(ntt_b200_context ctx, int op, size_t *bytes) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require(bytes != nullptr && op >= NTT_B200_HOST_FORWARD && op <= NTT_B200_HOST_MULTIPLY,
+            "invalid host transform query");
+    *bytes = 2 * aligned_bytes(host_transform_slot_words(*ctx, op));
+  });
+}
+
+int ntt_b200_host_transform(ntt_b200_context ctx, int op, uint64_t *values, const uint64_t *right,
+                            const uint32_t *tower_ids, size_t towers, void *workspace, size_t ws_size,
+                            void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    Ctx &c = *ctx;
+    require(op >= NTT_B200_HOST_FORWARD && op <= NTT_B200_HOST_MULTIPLY, "unknown host transform");
+    require(values && tower_ids, "null pointer");
+    const bool two = op >= NTT_B200_HOST_POINTWISE;
+    require(!two || right, "the product needs a right operand");
+    require(towers >= 1 && towers <= (size_t)b200::kMaxTowers, "host transform tower count out of range");
+    std::vector<uint16_t> ids(towers);
+    for (size_t i = 0; i < towers; ++i) {
+      require(tower_ids[i] < c.towers(), "tower id out of range");
+      ids[i] = (uint16_t)tower_ids[i];
+    }
+    require_aligned({workspace});
+    const size_t slot_words = host_transform_slot_words(c, op);
+    if (!workspace || ws_size < 2 * aligned_bytes(slot_words)) throw WorkspaceError("workspace missing or too small");
+    validate_host_values(c, values, ids);
+    if (two) validate_host_values(c, right, ids);
+    DeviceGuard guard(c.device);
+    std::lock_guard<std::mutex> lock(c.pipe_mu);
+    ensure_copy_pipeline(c);
+    const cudaStream_t st = as_stream(stream);
+    const size_t n = c.n;
+    char *base = reinterpret_cast<char *>(workspace);
+    u64 *slot[2] = {reinterpret_cast<u64 *>(base), reinterpret_cast<u64 *>(base + aligned_bytes(slot_words))};
+    CUDA_CHECK(cudaEventRecord(c.ev_start, st));
+    CUDA_CHECK(cudaStreamWaitEvent(c.copy_in, c.ev_start, 0));
+    CUDA_CHECK(cudaStreamWaitEvent(c.copy_out, c.ev_start, 0));
+    for (size_t first = 0, k = 0; first < towers; first += kHostChunkTowers, ++k) {
+      const size_t r = std::min(kHostChunkTowers, towers - first);
+      const int sl = (int)(k & 1);
+      u64 *d_l = slot[sl], *d_r = d_l + kHostChunkTowers * n;
+      // host -> device, once the transforms two chunks back have read this slot
+      CUDA_CHECK(cudaStreamWaitEvent(c.copy_in, c.ev_comp[sl], 0));
+      CUDA_CHECK(cudaMemcpyAsync(d_l, values + first * n, r * n * sizeof(u64), cudaMemcpyHostToDevice, c.copy_in));
+      if (two)
+        CUDA_CHECK(cudaMemcpyAsync(d_r, right + first * n, r * n * sizeof(u64), cudaMemcpyHostToDevice, c.copy_in));
+      CUDA_CHECK(cudaEventRecord(c.ev_in[sl], c.copy_in));
+      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_in[sl], 0));
+      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[sl], 0));
+      std::vector<Slot> slots;
+      for (size_t i = 0; i < r; ++i) slots.push_back({(uint32_t)i, ids[first + i]});
+      const u64 stride = r * n;
+      switch (op) {
+        case NTT_B200_HOST_FORWARD: run_ntt(c, d_l, d_l, slots, 1, stride, stride, false, st); break;
+        case NTT_B200_HOST_INVERSE: run_ntt(c, d_l, d_l, slots, 1, stride, stride, true, st); break;
+        case NTT_B200_HOST_POINTWISE: launch_pointwise(c, d_l, d_l, d_r, slots, st); break;
+        default:  // the ring product: forward both, pointwise, inverse
+          run_ntt(c, d_l, d_l, slots, 1, stride, stride, false, st);
+          run_ntt(c, d_r, d_r, slots, 1, stride, stride, false, st);
+          launch_pointwise(c, d_l, d_l, d_r, slots, st);
+          run_ntt(c, d_l, d_l, slots, 1, stride, stride, true, st);
+          break;
+      }
+      CUDA_CHECK(cudaEventRecord(c.ev_comp[sl], st));
+      CUDA_CHECK(cudaStreamWaitEvent(c.copy_out, c.ev_comp[sl], 0));
+      CUDA_CHECK(cudaMemcpyAsync(values + first * n, d_l, r * n * sizeof(u64), cudaMemcpyDeviceToHost, c.copy_out));
+      CUDA_CHECK(cudaEventRecord(c.ev_out[sl], c.copy_out));
+    }
+    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[0], 0));
+    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[1], 0));
+    CUDA_CHECK(cudaStreamSynchronize(st));  // synchronous, as the reference's public calls are
+  });
+}
+
+// ---- device arithmetic probes and test hooks -----------------------------------------------
+int ntt_b200_arith_probe(int device, int op, const uint64_t *queries, size_t count, uint64_t *out, void *stream) {
+  return guarded([&] {
+    require(op >= 0 && op <= 2, "unknown arithmetic probe");
+    require(queries && out && device >= 0, "null pointer");
+    require(count >= 1 && count <= (size_t(1) << 30), "probe count out of range");
+    DeviceGuard guard(device);
+    const cudaStream_t st = as_stream(stream);
+    Timed t("probe", st);
+    b200::arith_probe_kernel<<<(unsigned)((count + b200::kEwThreads - 1) / b200::kEwThreads), b200::kEwThreads, 0,
+                               st>>>(op, queries, count, out);
+    t.done();
+  });
+}
+
+int ntt_b200_conv_wait_polls(int polls) {
+  return guarded([&] {
+    require(polls >= 0 && polls <= (1 << 20), "poll limit out of range");
+    g_conv_first_wait = polls;
+  });
+}
+
+int ntt_b200_inject_setup_failure(size_t operation) {
+  g_setup_fail_at = operation;
+  return NTT_B200_OK;
+}
+
+int ntt_b200_setup_operations(size_t *count) {
+  return guarded([&] {
+    require(count != nullptr, "null output");
+    *count = g_setup_operations.load();
   });
 }
 }  // extern "C"

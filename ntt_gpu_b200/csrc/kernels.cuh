@@ -200,6 +200,7 @@ struct ConvTcArgs {
   uint16_t slot[kMaxConvTargets];
   int logn, kpad, groups;
   int tiles_per_cta;  // coefficient tiles per CTA (B, TMEM and barriers set up once per CTA)
+  int first_wait_polls;  // poll limit of the first bounded wait (for B); the others use kTcWaitPolls
   int *err;
 };
 
@@ -227,10 +228,12 @@ __host__ __device__ __forceinline__ int tc_canon(int r, int k, int rows) {
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-// Bounded wait for the completion of the mbarrier phase with the given parity.
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait for the completion of the mbarrier phase with the given parity:
+// at most `polls` polls (0 gives up at once).
+constexpr int kTcWaitPolls = 1 << 20;
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, int polls = kTcWaitPolls) {
   uint32_t got = 0;
-  for (int it = 0; it < (1 << 20) && !got; ++it)
+  for (int it = 0; it < polls && !got; ++it)
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
     // Every thread has read the staged rows: bring in the next tile's.
     if (ti + 1 < a.tiles_per_cta && tile + 1 < tiles) stage_tile(tile + 1);
     if (ti == 0) {  // B must have landed before the first MMA reads it
-      if (!__syncthreads_and(tc_wait(smem_addr(&bbar), 0))) {
+      if (!__syncthreads_and(tc_wait(smem_addr(&bbar), 0, a.first_wait_polls))) {
         ok = false;
         break;
       }
@@ -763,6 +766,25 @@ struct Words {
 template <int WORDS>
 __global__ void put_words(Words<WORDS> p, u64 *dst) {
   for (uint32_t i = threadIdx.x; i < p.count; i += blockDim.x) dst[i] = p.w[i];
+}
+
+// ---- device arithmetic probes ------------------------------------------------------
+// One query per thread (5 words each), as the reference probes its device
+// arithmetic against host 128-bit arithmetic (tests/basis_cuda.cu:49-65):
+//   op 0: (x, w, w', q)          -> x * w mod q, Shoup, canonical;
+//   op 1: (a, b, q, mu_lo, mu_hi) -> a * b mod q, Barrett with mu = floor(2^128 / q);
+//   op 2: (x, w, w', q)          -> the NTT's approximate-quotient Shoup product, in [0, 4q).
+static __global__ void __launch_bounds__(kEwThreads) arith_probe_kernel(int op, const u64 *queries, u64 count, u64 *out) {
+  const u64 i = u64(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const u64 *qr = queries + 5 * i;
+  if (op == 0) {
+    out[i] = shoup_canon(qr[0], qr[1], qr[2], qr[3]);
+  } else if (op == 1) {
+    out[i] = barrett_mul(qr[0], qr[1], Barrett{qr[2], qr[3], qr[4]});
+  } else {
+    out[i] = shoup_approx(qr[0], qr[1], qr[2], 0 - qr[3]);
+  }
 }
 
 // ---- pointwise product ------------------------------------------------------------

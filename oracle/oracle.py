@@ -32,7 +32,8 @@ def _ptr(a: np.ndarray | None):
 
 
 def build(force: bool = False) -> None:
-    """Compile liboracle.so (and oracle/_ref, CPU and CUDA, when the reference tree exists)."""
+    """Compile liboracle.so (and oracle/_ref - the reference CPU library, its CUDA path and its
+    Session over the B200 binding - when the reference tree exists)."""
     target = os.path.join(HERE, "liboracle.so")
     if force or not os.path.exists(target):
         subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
@@ -43,6 +44,10 @@ def build(force: bool = False) -> None:
     ref_cuda = os.path.join(HERE, "_ref", "libntt_ref_cuda.so")
     if (force or not os.path.exists(ref_cuda)) and shutil.which("nvcc"):
         subprocess.run(["make", "-s", "-C", HERE, "refcuda"], check=True)
+    # The reference's own Session over this repository's Driver binding (needs libntt_b200.so).
+    ref_b200 = os.path.join(HERE, "_ref", "libntt_ref_b200.so")
+    if force or not os.path.exists(ref_b200):
+        subprocess.run(["make", "-s", "-C", HERE, "refb200"], check=True)
 
 
 class _Ctx(ctypes.Structure):

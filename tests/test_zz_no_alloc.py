@@ -6,8 +6,10 @@ that cannot afford cudaMalloc's implicit device synchronisation, and an FFI
 host with no way to own device buffers across the boundary. This entry point
 serves them: its scratch is a fixed device array inside the library. The test
 checks, on two calls in a row, that its output equals the workspace-based
-ntt_b200_mod_down bit for bit. It also checks that a request larger than the
-array is refused before anything runs. The file is named to be collected last.
+ntt_b200_mod_down bit for bit, and that the second call leaves the device's
+free memory and its stream-ordered pool's usage unchanged (it allocates
+nothing). It also checks that a request larger than the array is refused
+before anything runs. The file is named to be collected last.
 """
 import ctypes
 
@@ -32,20 +34,35 @@ def _static_mod_down(g, level, dst, src):
     return rc, lib.ntt_b200_last_error().decode()
 
 
+def _device_memory():
+    """(free bytes of the device, bytes in use in its stream-ordered pool)."""
+    import torch
+    from cuda.bindings import runtime as rt
+    torch.cuda.synchronize()
+    err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
+    assert err == rt.cudaError_t.cudaSuccess
+    err, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    assert err == rt.cudaError_t.cudaSuccess
+    return torch.cuda.mem_get_info()[0], int(used)
+
+
 def _check_two_calls(orc, ctx, level, seeds):
     import torch
     g = nb.Context.from_oracle(ctx)
     g.prepare(level)
     ws = g.workspace(nb.OP_MOD_DOWN, level)
-    for seed in seeds:  # two calls in a row share (and overwrite) the static scratch
+    for call, seed in enumerate(seeds):  # two calls in a row share (and overwrite) the static scratch
         y = orc.lcg(ctx.n, ctx.qp_moduli(level), seed)
         src = nb.to_device(y)
         want = nb.empty((level, ctx.n))
         g.mod_down(level, want, src, ws)
         got = nb.empty((level, ctx.n))
+        before = _device_memory()
         rc, msg = _static_mod_down(g, level, got, src)
         assert rc == nb.OK, msg
         torch.cuda.synchronize()
+        if call > 0:  # after the first call's one-time set-up, a call allocates nothing
+            assert _device_memory() == before
         np.testing.assert_array_equal(nb.to_host(got), nb.to_host(want))
         np.testing.assert_array_equal(nb.to_host(got), orc.mod_down(ctx, level, y))
     g.close()
