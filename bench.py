@@ -666,23 +666,25 @@ def run_ours(args, rank, world, local):
     value = B * args.steps * world / (ms / 1000.0)
 
     # ---- roofline: the dominant kernel class of the step ------------------------------------------------
-    # Algorithmic bytes per step and class (W = 8N per tower; tables excluded). An NTT pass is half of a
-    # tower-transform, so each pass is credited W per tower (the transform's 2W split over its two passes).
-    # The fused row pass + key multiplication moves the digits' column-pass outputs, the input's own towers,
-    # the shared key rows once and both output channels. A conversion moves its s sources and t targets.
+    # Algorithmic bytes per step and class: each kernel's own input and output words (W = 8N per tower;
+    # twiddle, Shoup and CRT tables excluded). A two-pass NTT writes its intermediate in the first pass and
+    # reads it in the second, so each pass reads and writes every tower once; the ModDown row pass also reads
+    # the epilogue's operand. The fused row pass + key multiplication reads the digits' column-pass outputs,
+    # the input's own towers and the shared key rows once, and writes both output channels. A conversion
+    # reads its s sources and writes its t targets.
     W = 8 * N
     fused = "row_mac" in kernels
-    digit_towers = B * (beta * T - LEVEL)          # digit towers each input transforms
+    digit_towers = B * (beta * T - LEVEL)          # digit towers the inputs transform
     fwd_towers_per_step = digit_towers + 2 * B * LEVEL
     inv_towers_per_step = B * (LEVEL + 2 * K_P)
     bytes_per_step = {
-        "ntt_fwd_col": fwd_towers_per_step * W,
-        "ntt_fwd_row": (2 * B * LEVEL + (0 if fused else digit_towers)) * W,
-        "ntt_inv_row": inv_towers_per_step * W,
-        "ntt_inv_col": inv_towers_per_step * W,
+        "ntt_fwd_col": 2 * fwd_towers_per_step * W,
+        "ntt_fwd_row": (3 * 2 * B * LEVEL + (0 if fused else 2 * digit_towers)) * W,
+        "ntt_inv_row": 2 * inv_towers_per_step * W,
+        "ntt_inv_col": 2 * inv_towers_per_step * W,
         "conv": (beta * B * T + 2 * B * (K_P + LEVEL)) * W,
         "row_mac": (digit_towers + B * LEVEL + 2 * beta * T + 2 * B * T) * W,
-        "mac": (B * beta * T + B * LEVEL + 2 * beta * T + 2 * B * T) * W,
+        "mac": (digit_towers + B * LEVEL + 2 * beta * T + 2 * B * T) * W,
     }
     peak, peak_kind = peaks()
     classes = {}

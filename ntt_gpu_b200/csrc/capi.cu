@@ -2227,18 +2227,19 @@ size_t host_transform_slot_words(const Ctx &c, int op) {
 
 // Every residue below its tower's modulus (the reference's validate_values),
 // on the host before anything is enqueued; large inputs are split over threads.
+// With q < 2^63, x < q exactly when neither x nor (q - 1 - x) mod 2^64 has its
+// top bit set, so the scan is a subtraction and two ORs per word, which the
+// compiler vectorises.
 void validate_host_values(const Ctx &c, const u64 *v, const std::vector<uint16_t> &ids) {
   const size_t n = c.n, towers = ids.size();
   auto scan = [&](size_t t0, size_t t1) {
-    bool ok = true;
+    u64 flags = 0;
     for (size_t t = t0; t < t1; ++t) {
-      const u64 q = c.mod[ids[t]];
+      const u64 qm1 = c.mod[ids[t]] - 1;
       const u64 *p = v + t * n;
-      u64 bad = 0;
-      for (size_t i = 0; i < n; ++i) bad |= u64(p[i] >= q);
-      ok = ok && bad == 0;
+      for (size_t i = 0; i < n; ++i) flags |= (qm1 - p[i]) | p[i];
     }
-    return ok;
+    return (flags >> 63) == 0;
   };
   const size_t threads = std::min<size_t>(towers, towers * n >= (size_t(1) << 20) ? 8 : 1);
   bool ok = true;
