@@ -91,6 +91,30 @@ __device__ __forceinline__ void ct_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 
   }
 }
 
+// Forward butterflies without any reduction, for moduli q < 2^57 (a mode-2
+// context's towers below that size; the Q towers of the benchmark contexts
+// are 55-bit). With t = the approximate-quotient product in [0, 4q):
+//   x' = x + t, y' = x + 4q - t,
+// so from inputs in [0, R) both outputs lie in [0, R + 4q): the range grows by
+// 4q per stage. A forward transform starts below 4q and runs at most 16
+// stages, so every value stays below 68q < 2^63 for q < 2^57, and the
+// products accept any 64-bit input. The per-stage conditional subtraction of
+// ct_butterfly (most of its ALU work) disappears; the transform's consumer
+// reduces once (reduce_free_final) or takes the lazy values directly.
+constexpr u64 kFreeModulusBound = u64(1) << 57;
+constexpr int kFreeRangeFactor = 68;  // values stay below 68q
+template <bool FREE, int MODE, bool FRESH = false>
+__device__ __forceinline__ void ct_bf(u64 &x, u64 &y, u64 w, u64 wq, u64 q, u64 q2) {
+  if constexpr (FREE) {
+    const u64 t = shoup_approx(y, w, wq, 0 - q);
+    const u64 a = x;
+    x = a + t;
+    y = a + 2 * q2 - t;
+  } else {
+    ct_butterfly<MODE, FRESH>(x, y, w, wq, q, q2);
+  }
+}
+
 // Inverse Gentleman-Sande (x, y) -> (x + y, (x - y) * w). FRESH (mode 2): x and
 // y are canonical transform inputs, so x + y < 2q already lies in [0, 4q).
 template <int MODE, bool FRESH = false>
@@ -140,6 +164,15 @@ __device__ __forceinline__ u64 reduce_final(u64 x, u64 q, u64 q2) {
   if constexpr (MODE == 2) return csub_sign(csub_sign(csub_sign(x, 2 * q2), q2), q);
   else if constexpr (MODE == 1) return reduce4(x, q, q2);
   else return x;
+}
+
+// x mod m in [0, 4m) for any x < 2^64 and m < 2^62 (reduce64_approx is defined
+// below): the one reduction a reduction-free forward transform needs before a
+// consumer that wants [0, 4q), and with two subtractions more, canonical.
+__device__ __forceinline__ u64 reduce64_approx(u64 x, u64 one, u64 mneg);
+__device__ __forceinline__ u64 reduce_free_lazy(u64 x, u64 q, u64 one) { return reduce64_approx(x, one, 0 - q); }
+__device__ __forceinline__ u64 reduce_free_final(u64 x, u64 q, u64 one) {
+  return csub_sign(csub_sign(reduce64_approx(x, one, 0 - q), 2 * q), q);
 }
 
 // ---- 128-bit accumulation ------------------------------------------------------

@@ -504,7 +504,8 @@ int device_sms(int device) {
 // switch's plan) when the two-pass kernels run it.
 bool intt_unscaled(const Ctx &c) { return c.logn >= 12 && tuned("intt_unscaled") != 0; }
 // Hybrid digits that only feed the fused MAC stay in the forward NTT's lazy
-// range [0, 8q): with every modulus below 2^61 and at most 4 digits, the MAC's
+// range: [0, 8q), or [0, 68q) for towers below 2^57 (reduction-free forward
+// butterflies). With every modulus below 2^61 and at most 4 digits, the MAC's
 // 128-bit sums stay below 2^127 and its reductions give canonical results. The
 // 30-bit-limb MAC needs inputs below 2^60, so it rules this out.
 bool digits_lazy(const Ctx &c, size_t beta) {
@@ -997,10 +998,14 @@ void do_mac(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, u64 out_stri
           "rotation fused into the MAC needs its two-coefficient form and no accumulation");
   const b200::MacArgs a = mac_args(c, L, beta, out_b, out_a, out_stride, digits, digit_poly_stride, input, key_b,
                                    key_a, full_key_rows, accumulate, req, rot);
-  u64 max_q = 0;
-  for (auto q : c.mod) max_q = std::max(max_q, q);
-  // Lazy digits lie in [0, 8q).
-  const u128 prod = (u128)(lazy_digits ? 8 * max_q - 1 : max_q - 1) * (max_q - 1);
+  // Lazy digits lie in [0, 8q), or [0, 68q) for towers below 2^57 (reduction-free
+  // forward butterflies); the largest product of a digit and a key word decides
+  // whether beta of them can overflow 128 bits.
+  u128 prod = 0;
+  for (auto q : c.mod) {
+    const u64 range = !lazy_digits ? q : (q < b200::kFreeModulusBound ? b200::kFreeRangeFactor : 8) * q;
+    prod = std::max(prod, (u128)(range - 1) * (q - 1));
+  }
   const bool wide = prod > (~(u128)0) / (u128)beta;
   const bool limbs = mac_limbs_apply(c);
   require(!lazy_digits || (!limbs && beta <= 4 && n >= 2 * b200::kEwThreads), "lazy digits need the 2-coefficient MAC");

@@ -183,13 +183,13 @@ struct ColGeom {
 // inputs and store their outputs straight between registers and global memory
 // (coalesced 8-byte accesses) and use shared memory only for the exchange
 // between the two register phases.
-template <int LOGN, int MODE, int MINB, bool DIRECT>
-__global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
+// FREE: the reduction-free butterflies (ct_bf) for a tower with q < 2^57; the
+// pass then leaves its values below 4q + 4q * logR.
+template <int LOGN, int MODE, bool DIRECT, bool FREE>
+__device__ __forceinline__ void fwd_col_body(const NttBatch &b, const DeviceTables &T, u64 *tile, ulonglong2 *tw) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
   constexpr u64 kStride = N >> G::LR;
-  __shared__ __align__(16) u64 tile[kTileWords];
-  __shared__ ulonglong2 tw[G::R];
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int col0 = blockIdx.x * G::COLS;
@@ -217,9 +217,9 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
       // Stage 0 reads the transform's inputs, below 4q (canonical, or a
       // basis switch's lazy output), so mode 2 skips their first reduction.
       if (s == 0)
-        ct_butterfly<MODE, true>(x[e], x[e + d], w.x, w.y, q, q2);
+        ct_bf<FREE, MODE, true>(x[e], x[e + d], w.x, w.y, q, q2);
       else
-        ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+        ct_bf<FREE, MODE>(x[e], x[e + d], w.x, w.y, q, q2);
     }
   }
   if constexpr (G::LR > 4) {
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
         const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
-        ct_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+        ct_bf<FREE, MODE>(x[e], x[e + d], w.x, w.y, q, q2);
       }
     }
     if constexpr (DIRECT) {
@@ -262,6 +262,17 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
   }
   __syncthreads();
   store_block<G::R, G::COLS, G::COLS, false>(tower_dst(b, T, fresh_block_ids()) + col0, tile, kStride);
+}
+
+// The CTA's tower decides the butterflies: reduction-free below 2^57 (mode 2).
+template <int LOGN, int MODE, int MINB, bool DIRECT>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, DeviceTables T) {
+  __shared__ __align__(16) u64 tile[kTileWords];
+  __shared__ ulonglong2 tw[ColGeom<LOGN>::R];
+  if (MODE == 2 && T.tc[b.id[blockIdx.z]].q < kFreeModulusBound)
+    fwd_col_body<LOGN, MODE, DIRECT, MODE == 2>(b, T, tile, tw);
+  else
+    fwd_col_body<LOGN, MODE, DIRECT, false>(b, T, tile, tw);
 }
 
 // UNSCALED: the last stage is a plain Gentleman-Sande butterfly (no N^-1) and
@@ -413,13 +424,13 @@ __device__ __forceinline__ void ntt_copy16(void *smem, const void *gmem) {
                : "memory");
 }
 
-template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT, bool EPI_SMEM = false>
-__global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
-  static_assert(!(STW && DIRECT), "the staged-twiddle form has no direct variant");
-  static_assert(!EPI_SMEM || DIRECT, "the staged epilogue operand goes with the direct form");
+// FREE: the reduction-free butterflies for a tower with q < 2^57, continuing
+// from the column pass's values below 4q + 4q * logR; the outputs are then
+// reduced once (canonical, or [0, 4q) for the ModDown epilogue) or left below
+// 68q (lazy_out).
+template <int LOGN, int MODE, bool STW, bool DIRECT, bool EPI_SMEM, bool FREE>
+__device__ __forceinline__ void fwd_row_body(const NttBatch &b, const DeviceTables &T, u64 *tile, u64 *epi_rows) {
   constexpr int LR = LOGN - 8;
-  __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
-  extern __shared__ __align__(16) u64 epi_rows[];  // EPI_SMEM: 16 x 256 words of `left`
   const TowerView v = tower_view(b, T, false);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int row0 = blockIdx.x * 16;
@@ -465,7 +476,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
     for (int e = 0; e < 16; ++e) {
       if (e & d) continue;
       const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-      ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      ct_bf<FREE, MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
     }
   }
   __syncwarp();
@@ -487,7 +498,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
         const Shoup w = staged_twiddle(st, (r << sp) + row_lane_major(u, e >> (8 - sp)));
-        ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+        ct_bf<FREE, MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
     __syncthreads();  // staged twiddles read by every warp before the data returns
@@ -499,7 +510,7 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
         const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
-        ct_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+        ct_bf<FREE, MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
   }
@@ -507,10 +518,16 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
   // since the epilogue forms (left + 4q - x) * P^-1 and reduces that itself.
   const bool epi4 = MODE == 2 && b.epi_left != nullptr;
   const bool canonical = !b.lazy_out && !epi4;
+  const u64 one = v.c->red.one;
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
-    if (canonical) x[e] = reduce_final<MODE>(x[e], q, q2);
-    else if (epi4) x[e] = csub_sign(x[e], 2 * q2);
+    if constexpr (FREE) {
+      if (canonical) x[e] = reduce_free_final(x[e], q, one);
+      else if (epi4) x[e] = reduce_free_lazy(x[e], q, one);
+    } else {
+      if (canonical) x[e] = reduce_final<MODE>(x[e], q, q2);
+      else if (epi4) x[e] = csub_sign(x[e], 2 * q2);
+    }
     my[pad_col(u * 16 + e)] = x[e];
   }
   if constexpr (STW) {
@@ -568,6 +585,19 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
     }
     *reinterpret_cast<ulonglong2 *>(out + rr * 256 + c) = o;
   }
+}
+
+// The CTA's tower decides the butterflies: reduction-free below 2^57 (mode 2).
+template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT, bool EPI_SMEM = false>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, DeviceTables T) {
+  static_assert(!(STW && DIRECT), "the staged-twiddle form has no direct variant");
+  static_assert(!EPI_SMEM || DIRECT, "the staged epilogue operand goes with the direct form");
+  __shared__ __align__(16) u64 tile[STW ? kRowStwWords : 16 * kRowPad];
+  extern __shared__ __align__(16) u64 epi_rows[];  // EPI_SMEM: 16 x 256 words of `left`
+  if (MODE == 2 && T.tc[b.id[blockIdx.z]].q < kFreeModulusBound)
+    fwd_row_body<LOGN, MODE, STW, DIRECT, EPI_SMEM, MODE == 2>(b, T, tile, epi_rows);
+  else
+    fwd_row_body<LOGN, MODE, STW, DIRECT, EPI_SMEM, false>(b, T, tile, epi_rows);
 }
 
 template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT>

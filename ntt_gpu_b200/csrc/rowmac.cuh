@@ -24,9 +24,10 @@
 // the P towers (beta digits) run as two launches with their own region counts,
 // so the common Q towers fit three CTAs per SM at beta = 3.
 // Arithmetic: every modulus below 2^61 (butterfly mode 2). Digits stay in the
-// butterflies' lazy range [0, 8q); keys and the input are canonical, so with
-// at most 4 digits the sums stay below 4 * 8q * q < 2^127 and the
-// approximate-quotient reduction (reduce128_approx) applies.
+// butterflies' lazy range: [0, 8q), or [0, 68q) for towers below 2^57 whose
+// butterflies skip the per-stage reduction; keys and the input are canonical,
+// so with at most 4 digits the sums stay below max(4 * 8q * q, 4 * 68q * q)
+// < 2^127 and the approximate-quotient reduction (reduce128_approx) applies.
 #pragma once
 #include <cstdint>
 
@@ -63,12 +64,14 @@ __device__ __forceinline__ void rm_copy8(u64 *smem, const u64 *gmem) {
 // towers (t = blockIdx.z). The digits a CTA transforms run in order through
 // shared-memory regions 0, 1, ...; the rows of the next one are copied into
 // its region (cp.async) while the current one's butterflies run.
-template <int LOGN, int BETA, int WARPS, bool ROT, bool PT>
-__global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, DeviceTables T) {
+// FREE: reduction-free butterflies (ct_bf) for a tower with q < 2^57; its
+// digits then reach the key multiplication below 68q, and the sums stay below
+// 4 * 68q * q < 2^123.
+template <int LOGN, int BETA, int WARPS, bool ROT, bool PT, bool FREE>
+__device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTables &T, u64 *rm_digits) {
   constexpr int LR = LOGN - 8;
   constexpr u64 N = u64(1) << LOGN;
   constexpr int kRows = 2 * WARPS;  // rows per CTA
-  extern __shared__ __align__(16) u64 rm_digits[];  // [regions][kRows][kRowPad]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int h = lane >> 4, u = lane & 15;
   const int L = a.mac.level;
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, D
       for (int e = 0; e < 16; ++e) {
         if (e & dd) continue;
         const Shoup w = tw_load(tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-        ct_butterfly<2>(x[e], x[e + dd], w.w, w.wq, q, q2);
+        ct_bf<FREE, 2>(x[e], x[e + dd], w.w, w.wq, q, q2);
       }
     }
     __syncwarp();
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, D
       for (int e = 0; e < 16; ++e) {
         if (e & dd) continue;
         const Shoup w = tw_load(tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
-        ct_butterfly<2>(x[e], x[e + dd], w.w, w.wq, q, q2);
+        ct_bf<FREE, 2>(x[e], x[e + dd], w.w, w.wq, q, q2);
       }
     }
     // Each thread overwrites exactly the words it has just read: no barrier.
@@ -213,6 +216,17 @@ __global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, D
       }
     }
   }
+}
+
+// The CTA's tower decides the butterflies: reduction-free below 2^57.
+template <int LOGN, int BETA, int WARPS, bool ROT, bool PT>
+__global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, DeviceTables T) {
+  extern __shared__ __align__(16) u64 rm_digits[];  // [regions][2 * WARPS rows][kRowPad]
+  const int gid = PT ? a.mac.m + int(blockIdx.z) : int(blockIdx.z);
+  if (T.tc[gid].q < kFreeModulusBound)
+    row_mac_body<LOGN, BETA, WARPS, ROT, PT, true>(a, T, rm_digits);
+  else
+    row_mac_body<LOGN, BETA, WARPS, ROT, PT, false>(a, T, rm_digits);
 }
 
 }  // namespace b200

@@ -95,16 +95,29 @@ def test_batched_polys_with_stride(lib, orc):
         np.testing.assert_array_equal(got[p, len(q)], 0)  # the gap tower is untouched
 
 
-@pytest.mark.parametrize("bits", [[61], [62], [61, 62], [59, 61]])
+def primes_below(orc, n, count, bound):
+    """The largest NTT-friendly primes (q = 1 mod 2n) below `bound`."""
+    out, q = [], (bound - 1) // (2 * n) * (2 * n) + 1
+    while len(out) < count:
+        if q < bound and orc.is_prime(q):
+            out.append(q)
+        q -= 2 * n
+    return out
+
+
+@pytest.mark.parametrize("bits", [[61], [62], [61, 62], [59, 61], [-57], [58], [-57, 58], [30, 45, -57]])
 @pytest.mark.parametrize("logn", [12, 16])
 def test_butterfly_mode_boundaries(lib, orc, bits, logn):
     """Moduli just below 2^61 (fast approximate-quotient butterflies, values up to
-    8q), in [2^61, 2^62) (Harvey lazy butterflies) and mixed: exact results, with
-    all-(q-1) inputs driving every stage to the top of its range."""
+    8q), in [2^61, 2^62) (Harvey lazy butterflies), just below 2^57 (forward
+    butterflies without per-stage reductions, values up to 68q) and just above
+    it, and mixed within one launch: exact results, with all-(q-1) inputs
+    driving every stage to the top of its range."""
     n = 1 << logn
     q = []
-    for b in bits:
-        q += [v for v in orc.find_primes(n, 2, b) if v not in q][:2]
+    for b in bits:  # b < 0: the primes just below 2^|b|
+        found = primes_below(orc, n, 2, 1 << -b) if b < 0 else orc.find_primes(n, 2, b)
+        q += [v for v in found if v not in q][:2]
     psi = [orc.find_psi(v, n) for v in q]
     ctx = nb.Context(n, q, psi)
     ids = list(range(len(q)))

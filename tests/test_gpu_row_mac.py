@@ -86,3 +86,30 @@ def test_fused_request_list_with_shared_inputs(lib, orc):
         np.testing.assert_array_equal(nb.to_host(c.out_b), wb, err_msg=f"{c.kind} L={c.level}")
         np.testing.assert_array_equal(nb.to_host(c.out_a), wa, err_msg=f"{c.kind} L={c.level}")
     g.close()
+
+
+@pytest.mark.parametrize("n", [8192, 65536])
+def test_keyswitch_with_towers_at_the_reduction_free_bound(lib, orc, n):
+    """Q primes just below 2^57 (reduction-free forward butterflies at their
+    widest range, digits up to 68q into the key multiplication, and the ModDown
+    epilogue) next to 60-bit P primes (per-stage reductions) in the same
+    launches: key switch and rotation equal the oracle."""
+    from oracle.oracle import Context
+    from test_gpu_ntt import primes_below
+    q = primes_below(orc, n, 6, 1 << 57)
+    p = orc.find_primes(n, 3, 60)
+    ctx = Context(n, q, [orc.find_psi(v, n) for v in q], p, [orc.find_psi(v, n) for v in p], 2)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka, dkb, dka = _keys(orc, ctx, 97)
+    for level in (6, 3):
+        x = np.array([[v - 1] * n for v in ctx.q[:level]], dtype=np.uint64)  # top of every range
+        c0 = orc.lcg(n, ctx.q[:level], 5)
+        for rot in (False, True):
+            ob, oa = nb.empty((level, n)), nb.empty((level, n))
+            g.keyswitch(level, ob, oa, nb.to_device(x), dkb, dka, g.workspace(nb.OP_KEYSWITCH, level),
+                        c0=nb.to_device(c0) if rot else None, automorphism=25 if rot else 0)
+            _sync()
+            wb, wa = orc.keyswitch(ctx, level, x, kb, ka, c0 if rot else None, 25 if rot else 0)
+            np.testing.assert_array_equal(nb.to_host(ob), wb, err_msg=f"L={level} rot={rot}")
+            np.testing.assert_array_equal(nb.to_host(oa), wa, err_msg=f"L={level} rot={rot}")
+    g.close()
