@@ -166,11 +166,10 @@ __device__ __forceinline__ u64 reduce_final(u64 x, u64 q, u64 q2) {
   else return x;
 }
 
-// x mod m in [0, 4m) for any x < 2^64 and m < 2^62 (reduce64_approx is defined
-// below): the one reduction a reduction-free forward transform needs before a
-// consumer that wants [0, 4q), and with two subtractions more, canonical.
+// Canonical x mod q from a reduction-free forward transform's values (any
+// x < 2^64): reduce64_approx (defined below) brings x into [0, 4q), two
+// subtractions finish it.
 __device__ __forceinline__ u64 reduce64_approx(u64 x, u64 one, u64 mneg);
-__device__ __forceinline__ u64 reduce_free_lazy(u64 x, u64 q, u64 one) { return reduce64_approx(x, one, 0 - q); }
 __device__ __forceinline__ u64 reduce_free_final(u64 x, u64 q, u64 one) {
   return csub_sign(csub_sign(reduce64_approx(x, one, 0 - q), 2 * q), q);
 }

@@ -514,8 +514,9 @@ __device__ __forceinline__ void fwd_row_body(const NttBatch &b, const DeviceTabl
       }
     }
   }
-  // Mode 2 with the ModDown epilogue: the values only need to reach [0, 4q),
-  // since the epilogue forms (left + 4q - x) * P^-1 and reduces that itself.
+  // Mode 2 with the ModDown epilogue: the values only need to reach [0, 4q)
+  // (or stay below 68q after reduction-free butterflies), since the epilogue
+  // forms (left + span - x) * P^-1 and reduces that itself.
   const bool epi4 = MODE == 2 && b.epi_left != nullptr;
   const bool canonical = !b.lazy_out && !epi4;
   const u64 one = v.c->red.one;
@@ -523,7 +524,7 @@ __device__ __forceinline__ void fwd_row_body(const NttBatch &b, const DeviceTabl
   for (int e = 0; e < 16; ++e) {
     if constexpr (FREE) {
       if (canonical) x[e] = reduce_free_final(x[e], q, one);
-      else if (epi4) x[e] = reduce_free_lazy(x[e], q, one);
+      // the ModDown epilogue takes x below 68q directly (below)
     } else {
       if (canonical) x[e] = reduce_final<MODE>(x[e], q, q2);
       else if (epi4) x[e] = csub_sign(x[e], 2 * q2);
@@ -571,9 +572,11 @@ __device__ __forceinline__ void fwd_row_body(const NttBatch &b, const DeviceTabl
     if constexpr (MODE == 2) {
       // left < q and x < 4q: left + 4q - x lies in (0, 5q), below 2^64 for q < 2^61;
       // the approximate-quotient product lands in [0, 4q), two subtractions finish it.
-      const u64 q4 = 2 * q2, qneg = 0 - q;
-      o.x = csub_sign(csub_sign(shoup_approx(l.x + q4 - tile[sidx], pinv.w, pinv.wq, qneg), q2), q);
-      o.y = csub_sign(csub_sign(shoup_approx(l.y + q4 - tile[sidx + 1], pinv.w, pinv.wq, qneg), q2), q);
+      // x < 4q, or x < 68q after reduction-free butterflies: left + span - x
+      // lies in (0, span + q), below 2^64, and the product accepts any word.
+      const u64 span = FREE ? u64(kFreeRangeFactor) * q : 2 * q2, qneg = 0 - q;
+      o.x = csub_sign(csub_sign(shoup_approx(l.x + span - tile[sidx], pinv.w, pinv.wq, qneg), q2), q);
+      o.y = csub_sign(csub_sign(shoup_approx(l.y + span - tile[sidx + 1], pinv.w, pinv.wq, qneg), q2), q);
     } else {
       o.x = shoup_canon(sub_mod(l.x, tile[sidx], q), pinv.w, pinv.wq, q);
       o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
