@@ -670,17 +670,20 @@ def run_ours(args, rank, world, local):
     # twiddle, Shoup and CRT tables excluded). A two-pass NTT writes its intermediate in the first pass and
     # reads it in the second, so each pass reads and writes every tower once; the ModDown row pass also reads
     # the epilogue's operand. The fused row pass + key multiplication reads the digits' column-pass outputs,
-    # the input's own towers and the shared key rows once, and writes both output channels. A conversion
-    # reads its s sources and writes its t targets.
+    # the input's own towers and the shared key rows once, and writes both output channels; on the P towers
+    # it also runs the ModDown's inverse row pass before storing (no extra I/O), so the separate inverse row
+    # pass then only transforms the inputs. A conversion reads its s sources and writes its t targets.
     W = 8 * N
     fused = "row_mac" in kernels
+    p_rows_fused = fused and beta >= 2 and nb.tuning_get("row_mac_inv_rows") != 0
     digit_towers = B * (beta * T - LEVEL)          # digit towers the inputs transform
     fwd_towers_per_step = digit_towers + 2 * B * LEVEL
     inv_towers_per_step = B * (LEVEL + 2 * K_P)
+    inv_row_towers_per_step = B * LEVEL + (0 if p_rows_fused else 2 * B * K_P)
     bytes_per_step = {
         "ntt_fwd_col": 2 * fwd_towers_per_step * W,
         "ntt_fwd_row": (3 * 2 * B * LEVEL + (0 if fused else 2 * digit_towers)) * W,
-        "ntt_inv_row": 2 * inv_towers_per_step * W,
+        "ntt_inv_row": 2 * inv_row_towers_per_step * W,
         "ntt_inv_col": 2 * inv_towers_per_step * W,
         "conv": (beta * B * T + 2 * B * (K_P + LEVEL)) * W,
         "row_mac": (digit_towers + B * LEVEL + 2 * beta * T + 2 * B * T) * W,

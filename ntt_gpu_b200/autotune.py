@@ -102,6 +102,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("conv_tc_fixed", (0, 1), ks_step, ("conv",), {"conv_tc": 1}),
         ("conv_tc_tiles", (1, 2, 4, 8), ks_step, ("conv",), {"conv_tc": 1}),
         ("row_mac", (0, 1), ks_step, ("ntt_fwd_row", "mac", "row_mac"), {}),
+        ("row_mac_inv_rows", (0, 1), ks_step, ("row_mac", "ntt_inv_row"), {"row_mac": 1}),
     ]
     measurements, choices = {}, {}
     for name, candidates, step, kernels, pinned in plan:

@@ -470,8 +470,8 @@ Tunable g_tuning[] = {
     {"ntt_minb_inv_col", {4}, 3, 4},
     {"ntt_col_direct", {1}, 0, 1},     // column passes load and store between registers and global memory
     {"ntt_row_direct", {1}, 0, 1},     // row passes load (forward) / store (inverse) mapping A directly
-    {"intt_unscaled", {1}, 0, 1},
-    {"digits_lazy", {1}, 0, 1},        // Hybrid digits feeding the fused MAC skip their final reduction      // inverse NTTs feeding a basis switch leave N^-1 to the switch
+    {"intt_unscaled", {1}, 0, 1},      // inverse NTTs feeding a basis switch leave N^-1 to the switch
+    {"digits_lazy", {1}, 0, 1},        // Hybrid digits feeding the fused MAC skip their final reduction
     {"ntt_epi_stage", {0}, 0, 1},      // ModDown row pass stages its `left` rows in shared memory (measured slower)
     {"ntt_stage_tw_fwd_row", {0}, 0, 1},  // row passes stage their register-stage twiddles in shared memory
     {"ntt_stage_tw_inv_row", {0}, 0, 1},
@@ -485,6 +485,7 @@ Tunable g_tuning[] = {
     {"conv_tc_fixed", {1}, 0, 1},      // tensor-core conversion kernels compiled for 8 -> 24/16/8 towers
     {"row_mac", {1}, 0, 1},            // key multiplication fused into the digits' forward row pass
     {"row_mac_max_beta", {4}, 1, 4},   // largest digit count the fused row pass takes (shared memory per CTA grows with it)
+    {"row_mac_inv_rows", {1}, 0, 1},   // its P towers run the ModDown's inverse row pass before they are stored
 };
 Tunable *find_tunable(const char *name) {
   for (auto &t : g_tuning)
@@ -526,14 +527,18 @@ void launch_fwd_row_epi(const Ctx &c, const b200::NttBatch &b, dim3 grid, cudaSt
   kernel<<<grid, b200::kNttThreads, b200::kEpiSmemBytes, st>>>(b, c.tables);
 }
 
+// row_done (inverse): the row pass has run already (inside the fused row pass +
+// key multiplication), so the column pass reads the source directly.
 template <int LOGN, int MODE>
 void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
-                      bool inverse, cudaStream_t st, bool col_only) {
+                      bool inverse, cudaStream_t st, bool col_only, bool row_done) {
   const dim3 grid((1u << LOGN) / b200::kTileWords, polys, slots);
   b200::NttBatch second = b;
-  second.src = b.dst;
-  second.src_stride = b.dst_stride;
-  second.src_list = nullptr;
+  if (!row_done) {
+    second.src = b.dst;
+    second.src_stride = b.dst_stride;
+    second.src_list = nullptr;
+  }
   if (fin) {
     second.dst = fin->dst;
     second.dst_odd = fin->dst_odd;
@@ -573,14 +578,16 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
       NTT_LAUNCH(fwd_row, second, false, false);
     t2.done();
   } else {
-    Timed t1("ntt_inv_row", st);
-    if (tuned("ntt_stage_tw_inv_row"))
-      NTT_LAUNCH(inv_row, b, true, false);
-    else if (tuned("ntt_row_direct"))
-      NTT_LAUNCH(inv_row, b, false, true);
-    else
-      NTT_LAUNCH(inv_row, b, false, false);
-    t1.done();
+    if (!row_done) {
+      Timed t1("ntt_inv_row", st);
+      if (tuned("ntt_stage_tw_inv_row"))
+        NTT_LAUNCH(inv_row, b, true, false);
+      else if (tuned("ntt_row_direct"))
+        NTT_LAUNCH(inv_row, b, false, true);
+      else
+        NTT_LAUNCH(inv_row, b, false, false);
+      t1.done();
+    }
     Timed t2("ntt_inv_col", st);
     if (second.unscaled) {
       if (tuned("ntt_col_direct"))
@@ -599,13 +606,13 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
 
 template <int MODE>
 void launch_ntt_chunk(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin, int slots, int polys,
-                      bool inverse, cudaStream_t st, bool col_only) {
+                      bool inverse, cudaStream_t st, bool col_only, bool row_done) {
   switch (c.logn) {
-    case 12: launch_ntt_2pass<12, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
-    case 13: launch_ntt_2pass<13, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
-    case 14: launch_ntt_2pass<14, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
-    case 15: launch_ntt_2pass<15, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
-    case 16: launch_ntt_2pass<16, MODE>(c, b, fin, slots, polys, inverse, st, col_only); break;
+    case 12: launch_ntt_2pass<12, MODE>(c, b, fin, slots, polys, inverse, st, col_only, row_done); break;
+    case 13: launch_ntt_2pass<13, MODE>(c, b, fin, slots, polys, inverse, st, col_only, row_done); break;
+    case 14: launch_ntt_2pass<14, MODE>(c, b, fin, slots, polys, inverse, st, col_only, row_done); break;
+    case 15: launch_ntt_2pass<15, MODE>(c, b, fin, slots, polys, inverse, st, col_only, row_done); break;
+    case 16: launch_ntt_2pass<16, MODE>(c, b, fin, slots, polys, inverse, st, col_only, row_done); break;
     default: throw ContractError("unsupported ring dimension");
   }
 }
@@ -622,13 +629,17 @@ dim3 ew_grid(const Ctx &c, size_t towers, size_t polys) {
 // src_list (device array, one entry per polynomial) replaces src / src_stride.
 // col_only (two-pass forward transforms, mode 2): run the column pass alone;
 // the fused row pass + key multiplication (ntt_fwd_row_mac) finishes it.
+// row_done (two-pass inverse transforms, mode 2): src has been through the
+// row pass already (the fused kernel's P towers); run the column pass alone.
 void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &slots_in, size_t polys,
              u64 src_stride, u64 dst_stride, bool inverse, cudaStream_t st, const NttFinal *fin = nullptr,
              const u64 *const *src_list = nullptr, bool unscaled = false, bool lazy_out = false,
-             bool col_only = false) {
+             bool col_only = false, bool row_done = false) {
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   require(!col_only || (!inverse && !fin && c.logn >= 12 && c.mode == 2),
           "a column pass alone is a two-pass mode-2 forward transform");
+  require(!row_done || (inverse && !src_list && c.logn >= 12 && c.mode == 2),
+          "a transform from its column pass is a two-pass mode-2 inverse");
   require(!fin || !inverse, "final-pass redirection is forward only");
   require(!unscaled || (inverse && c.logn >= 12), "unscaled transforms are two-pass inverses only");
   require(!lazy_out || (!inverse && !fin && c.logn >= 12), "lazy outputs are two-pass forward transforms only");
@@ -684,11 +695,11 @@ void run_ntt(const Ctx &c, u64 *dst, const u64 *src, const std::vector<Slot> &sl
         t.done();
       }
     } else if (c.mode == 2) {
-      launch_ntt_chunk<2>(c, b, fin, (int)count, (int)polys, inverse, st, col_only);
+      launch_ntt_chunk<2>(c, b, fin, (int)count, (int)polys, inverse, st, col_only, row_done);
     } else if (c.mode == 1) {
-      launch_ntt_chunk<1>(c, b, fin, (int)count, (int)polys, inverse, st, false);
+      launch_ntt_chunk<1>(c, b, fin, (int)count, (int)polys, inverse, st, false, false);
     } else {
-      launch_ntt_chunk<0>(c, b, fin, (int)count, (int)polys, inverse, st, false);
+      launch_ntt_chunk<0>(c, b, fin, (int)count, (int)polys, inverse, st, false, false);
     }
   }
 }
@@ -852,15 +863,17 @@ Carver carve(const Ctx &c, void *ws, size_t bytes, int op, size_t level, size_t 
 // evaluation Q_L (stride dst_stride, or split even/odd destinations).
 // dst_list / add_list (device arrays, one entry per polynomial) optionally
 // redirect each output and add a per-polynomial addend.
+// p_rows_done: the P towers of src have been through the inverse NTT's row
+// pass already (the fused row pass + key multiplication ran it).
 void do_mod_down(Ctx &c, size_t L, size_t polys, u64 *dst, u64 *dst_odd, u64 dst_stride, const u64 *src,
                  u64 src_stride, Carver &ws, cudaStream_t st, u64 *const *dst_list = nullptr,
-                 const u64 *const *add_list = nullptr) {
+                 const u64 *const *add_list = nullptr, bool p_rows_done = false) {
   const size_t n = c.n, K = c.k;
   u64 *p_coeff = ws.take(polys * K * n);
   u64 *corr = ws.take(polys * L * n);
   const bool unscaled = intt_unscaled(c);
   run_ntt(c, p_coeff, src + L * n, contiguous_slots(range_ids(c.m, c.m + K)), polys, src_stride, K * n,
-          true, st, nullptr, nullptr, unscaled);
+          true, st, nullptr, nullptr, unscaled, false, false, p_rows_done);
   const auto &plan = c.conv_plan(range_ids(c.m, c.m + K), range_ids(0, L), unscaled);
   std::vector<uint16_t> slots;
   for (size_t i = 0; i < L; ++i) slots.push_back((uint16_t)i);
@@ -1070,14 +1083,24 @@ bool row_mac_applies(const Ctx &c, size_t L) {
          beta <= (size_t)std::min<int64_t>(tuned("row_mac_max_beta"), b200::kRowMacMaxBeta);
 }
 
+// Whether the fused kernel's P towers also run the ModDown's inverse row pass:
+// two digits or more (their regions hold the two channels) and one request per
+// input (hoisted requests still need the digits after the first request).
+bool row_mac_inv_rows_applies(const Ctx &c, size_t L, bool one_request_per_input) {
+  const size_t beta = 1 + (L - 1) / c.alpha;
+  return one_request_per_input && beta >= 2 && tuned("row_mac_inv_rows") != 0;
+}
+
 // The fused row pass + key multiplication over `inputs` distinct inputs whose
 // digits have been through their forward column pass (digits + u * beta*T*N).
 // Strided mode (req == nullptr): request u is input u, with the shared
 // full-context key and, with rot.on, c0 + u * rot.c0_stride. Request-table
 // mode: input u serves requests [first, first + count) of `groups`.
+// p_inverse_rows: the P towers' outputs leave through the ModDown's inverse row
+// pass (row_mac_inv_rows applies).
 void do_row_mac(Ctx &c, size_t L, size_t inputs, u64 *out_b, u64 *out_a, u64 out_stride, const u64 *digits,
                 const u64 *input, const u64 *key_b, const u64 *key_a, const b200::ReqDesc *req, const u64 *groups,
-                const MacRotation &rot, cudaStream_t st) {
+                const MacRotation &rot, cudaStream_t st, bool p_inverse_rows = false) {
   const size_t n = c.n, T = L + c.k, beta = 1 + (L - 1) / c.alpha;
   require(inputs >= 1 && inputs <= 65535, "request batch out of range");
   std::vector<const u64 *> kb, ka;
@@ -1091,6 +1114,7 @@ void do_row_mac(Ctx &c, size_t L, size_t inputs, u64 *out_b, u64 *out_a, u64 out
   a.digit_stride = beta * T * n;
   a.groups = groups;
   a.towers = (int)T;
+  a.p_inverse_rows = p_inverse_rows;
   Timed t("row_mac", st);
   CUDA_CHECK(b200::row_mac_launch(a, c.tables, c.logn, (int)beta, rot.on, (unsigned)inputs, (unsigned)T, st));
   t.done();
@@ -1131,10 +1155,11 @@ void do_keyswitch(Ctx &c, size_t L, size_t batch, u64 *out_b, u64 *out_a, const 
   u64 *rot = ws.take(2 * batch * T * n);
   if (c0) require((g & 1) && g < 2 * c.n, "invalid negacyclic automorphism index");
   if (row_mac_applies(c, L)) {
+    const bool inv_rows = row_mac_inv_rows_applies(c, L, true);
     do_digits(c, L, batch, digits, src, ws, false, st, nullptr, true, true);
     do_row_mac(c, L, batch, acc, acc + T * n, 2 * T * n, digits, src, key_b, key_a, nullptr, nullptr,
-               MacRotation{c0 != nullptr, c0, L * n, g}, st);
-    do_mod_down(c, L, 2 * batch, out_b, out_a, L * n, acc, T * n, ws, st);
+               MacRotation{c0 != nullptr, c0, L * n, g}, st, inv_rows);
+    do_mod_down(c, L, 2 * batch, out_b, out_a, L * n, acc, T * n, ws, st, nullptr, nullptr, inv_rows);
     return;
   }
   const bool lazy = digits_lazy(c, beta);
@@ -1283,10 +1308,12 @@ void run_chunk(Ctx &c, const ntt_b200_ks_request *reqs, const Chunk &ch, Carver 
   u64 *digits = ws.take(u * beta * T * n);
   u64 *acc = ws.take(2 * r * T * n);  // [request][b|a][T][N]
   if (row_mac_applies(c, L)) {
+    const bool inv_rows = row_mac_inv_rows_applies(c, L, u == r);
     do_digits(c, L, u, digits, nullptr, ws, false, st, usrc, true, true);
     do_row_mac(c, L, u, acc, acc + T * n, 2 * T * n, digits, nullptr, nullptr, nullptr, desc, groups,
-               MacRotation{ch.rotate}, st);
-    do_mod_down(c, L, 2 * r, nullptr, nullptr, 0, acc, T * n, ws, st, dst_list, ch.add ? add_list : nullptr);
+               MacRotation{ch.rotate}, st, inv_rows);
+    do_mod_down(c, L, 2 * r, nullptr, nullptr, 0, acc, T * n, ws, st, dst_list, ch.add ? add_list : nullptr,
+                inv_rows);
     return;
   }
   const bool fused = ch.rotate && mac_fuses_rotation(c, L);

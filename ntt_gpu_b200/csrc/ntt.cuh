@@ -603,6 +603,50 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
     fwd_row_body<LOGN, MODE, STW, DIRECT, EPI_SMEM, false>(b, T, tile, epi_rows);
 }
 
+// The inverse row pass's butterflies (stages logR + 7 .. logR, Gentleman-Sande)
+// on row `row` of a tower, by the 16 threads u = 0..15 of that row, with every
+// twiddle read from global memory. On entry x[e] holds the row's word u*16 + e
+// (canonical: the first stage adds without reducing); on exit x[e] holds its
+// word e*16 + u. `my` is the row's padded shared-memory buffer, used for the
+// exchange between the two register phases; the row's threads may still be
+// reading it on entry (the exchange starts with __syncwarp).
+template <int LOGN, int MODE>
+__device__ __forceinline__ void inv_row_stages(u64 (&x)[16], u64 *my, const ulonglong2 *tw, int row, int u, u64 q,
+                                               u64 q2) {
+  constexpr int LR = LOGN - 8;
+  // Stages LR + s', s' = 7..4: column bit 7-s' == register bit 7-s'.
+#pragma unroll
+  for (int sp = 7; sp >= 4; --sp) {
+    const int s = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
+      if (sp == 7)
+        gs_butterfly<MODE, true>(x[e], x[e + d], w.w, w.wq, q, q2);
+      else
+        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+  // Stages LR + s', s' = 3..0: column bit 7-s' == register bit 3-s'.
+#pragma unroll
+  for (int sp = 3; sp >= 0; --sp) {
+    const int s = LR + sp, d = 8 >> sp;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
+      gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+}
+
 template <int LOGN, int MODE, int MINB, bool STW, bool DIRECT>
 __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, DeviceTables T) {
   static_assert(!(STW && DIRECT), "the staged-twiddle form has no direct variant");
@@ -624,8 +668,8 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
   u64 x[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
-  // Stages LR + s', s' = 7..4: column bit 7-s' == register bit 7-s'.
   if constexpr (STW) {
+    // Stages LR + s', s' = 7..4, twiddles staged in shared memory per stage.
     ulonglong2 *st = reinterpret_cast<ulonglong2 *>(tile);
 #pragma unroll
     for (int sp = 7; sp >= 4; --sp) {
@@ -641,38 +685,24 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
       }
     }
     __syncthreads();  // staged twiddles read by every warp before the data returns
-  } else {
+    __syncwarp();
 #pragma unroll
-    for (int sp = 7; sp >= 4; --sp) {
-      const int s = LR + sp, d = 1 << (7 - sp);
+    for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+#pragma unroll
+    for (int sp = 3; sp >= 0; --sp) {
+      const int s = LR + sp, d = 8 >> sp;
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
-        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
-        // The first stage reads the inverse transform's canonical inputs.
-        if (sp == 7)
-          gs_butterfly<MODE, true>(x[e], x[e + d], w.w, w.wq, q, q2);
-        else
-          gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+        const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
+        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
-  __syncwarp();
-#pragma unroll
-  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
-  // Stages LR + s', s' = 3..0: column bit 7-s' == register bit 3-s'.
-#pragma unroll
-  for (int sp = 3; sp >= 0; --sp) {
-    const int s = LR + sp, d = 8 >> sp;
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      if (e & d) continue;
-      const Shoup w = tw_load(v.tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-      gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
-    }
+  } else {
+    inv_row_stages<LOGN, MODE>(x, my, v.tw, row, u, q, q2);
   }
   if constexpr (DIRECT) {
     u64 *const out = tower_dst(b, T, fresh_block_ids()) + row * 256 + u;

@@ -17,6 +17,16 @@
 // the automorphism moves it to; resident_hybrid_rotate_kernel of
 // src/cuda/resident_adapter.inc:44-59).
 //
+// On the P towers the ModDown starts right away (p_inverse_rows): the MAC
+// leaves both channels' values in shared memory, over the digit words it has
+// just read, and the inverse NTT's row pass (Session::mod_down's transform,
+// src/resident.cpp:448-457) runs on them before anything is stored, so the P
+// part is written once, as that pass's output, instead of being written by
+// the MAC and read and rewritten by a separate row pass. A rotation moves whole
+// rows: the automorphism's source slot of destination row r_d lies in one row
+// r_s, which depends on r_d only, so the row pass of r_d gathers its 256 words
+// from row r_s of the CTA.
+//
 // Layout: each warp owns two rows through both register phases of every
 // digit's row pass and through the MAC, so the CTA never synchronises; its
 // dynamic shared memory holds one padded region of 2 * WARPS rows per digit it
@@ -44,6 +54,10 @@ struct RowMacArgs {
   u64 digit_stride;
   const u64 *groups;      // request-table mode: per distinct input, first request | count << 32
   int towers;             // L + K
+  // P towers, beta >= 2, one request per input: the P part of both channels
+  // goes through the ModDown's first pass (the inverse NTT's row pass) in
+  // shared memory and is stored as that pass's output.
+  bool p_inverse_rows;
 };
 
 // Shared memory of one launch: Q towers transform beta - 1 digits (their own
@@ -51,6 +65,15 @@ struct RowMacArgs {
 template <int WARPS>
 constexpr int row_mac_smem_bytes(int regions) {
   return regions * 2 * WARPS * kRowPad * int(sizeof(u64));
+}
+// CTAs per SM that a launch's shared memory allows (228 KiB per SM, 1 KiB of
+// it reserved per CTA), at most 3: the register bound of __launch_bounds__, so
+// that a launch whose shared memory admits fewer CTAs gets the registers.
+template <int WARPS>
+constexpr int row_mac_ctas_per_sm(int regions) {
+  const int per_cta = row_mac_smem_bytes<WARPS>(regions) + 1024;
+  const int fit = (228 * 1024) / per_cta;
+  return fit < 1 ? 1 : fit > 3 ? 3 : fit;
 }
 
 // 8-byte global -> shared copy that completes asynchronously (cp.async groups).
@@ -152,6 +175,9 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
   // Key multiplication over the warp's two rows: 2 adjacent coefficients per
   // lane and step, 16-byte loads of the input's own tower and of the keys.
   const Reducer red = tc->red;
+  // Two digit regions hold the two channels; the host sets p_inverse_rows
+  // only when every input serves one request (its digits are then dead).
+  const bool inv_rows = PT && BETA >= 2 && a.p_inverse_rows;
   u64 first = input, count = 1;
   if (a.groups) {
     const u64 gw = a.groups[input];
@@ -198,6 +224,17 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
       rb.y = reduce128_approx((u64)b1.v, (u64)(b1.v >> 64), red);
       ra.x = reduce128_approx((u64)a0.v, (u64)(a0.v >> 64), red);
       ra.y = reduce128_approx((u64)a1.v, (u64)(a1.v >> 64), red);
+      if (inv_rows) {
+        // Channel b over digit 0's words of these two slots, channel a over
+        // digit 1's: this lane has read them above and no other lane reads them.
+        u64 *sb = rm_digits + (2 * warp + rr) * kRowPad + pad_col(c);
+        u64 *sa = sb + kRows * kRowPad;
+        sb[0] = rb.x;
+        sb[1] = rb.y;
+        sa[0] = ra.x;
+        sa[1] = ra.y;
+        continue;
+      }
       if constexpr (ROT) {
         if (!PT && mb.c0) {  // rotated_b_value: b + P * c0 on the Q towers
           const ulonglong2 cc = *reinterpret_cast<const ulonglong2 *>(mb.c0 + u64(t) * N + i);
@@ -215,12 +252,54 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
         *reinterpret_cast<ulonglong2 *>(a.mac.out_a + obase + i) = ra;
       }
     }
+    if (inv_rows) {
+      // The inverse NTT's row pass of the warp's two destination rows per
+      // channel, 16 threads per row; with a rotation, destination row rd takes
+      // slot automorphism_source(rd * 256 + col, g) of source row `row`.
+      __syncwarp();
+      // In bit-reversed slot order (br_k: k-bit reversal, R = logN - 8 row bits)
+      // the automorphism moves source row `row` to destination row
+      //   rd = br_R((((2 br_R(row) + 1) g^-1) >> 1) mod 2^R),
+      // and destination word (rd, 16u + e) comes from column
+      //   br8((base + 16 * (br4(e) g mod 16)) mod 256) of row `row`, with
+      //   base = br4(u) g + (((2 br_R(rd) + 1) g mod 2N) >> (logN - 7))
+      // (automorphism_source written out in 32-bit arithmetic).
+      int rd = row;
+      uint32_t base = 0, g16 = 0;
+      if constexpr (ROT) {
+        constexpr int R = LOGN - 8;
+        const uint32_t rbr = __brev(uint32_t(row)) >> (32 - R);
+        rd = int(__brev((((2 * rbr + 1) * gi) >> 1) & ((1u << R) - 1)) >> (32 - R));
+        const uint32_t g = mb.g, dbr = __brev(uint32_t(rd)) >> (32 - R);
+        const uint32_t carry = (((2 * dbr + 1) * g) & uint32_t(2 * N - 1)) >> (LOGN - 7);
+        base = (__brev(uint32_t(u)) >> 28) * g + carry;
+        g16 = g & 15u;
+      }
+      const ulonglong2 *itw = T.inv + u64(gid) * N;
+#pragma unroll 1
+      for (int ch = 0; ch < 2; ++ch) {
+        u64 *my = rm_digits + (ch * kRows + 2 * warp + h) * kRowPad;
+        u64 x[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          constexpr uint32_t kBr4[16] = {0, 8, 4, 12, 2, 10, 6, 14, 1, 9, 5, 13, 3, 11, 7, 15};
+          const uint32_t cs =
+              ROT ? __brev((base + 16 * ((kBr4[e] * g16) & 15u)) & 255u) >> 24 : uint32_t(u * 16 + e);
+          x[e] = my[pad_col(int(cs))];
+        }
+        inv_row_stages<LOGN, 2>(x, my, itw, rd, u, q, q2);
+        u64 *o = (ch == 0 ? a.mac.out_b : a.mac.out_a) + obase + u64(rd) * 256 + u;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) o[e * 16] = x[e];
+      }
+    }
   }
 }
 
 // The CTA's tower decides the butterflies: reduction-free below 2^57.
 template <int LOGN, int BETA, int WARPS, bool ROT, bool PT>
-__global__ void __launch_bounds__(WARPS * 32, 3) ntt_fwd_row_mac(RowMacArgs a, DeviceTables T) {
+__global__ void __launch_bounds__(WARPS * 32, row_mac_ctas_per_sm<WARPS>(PT ? BETA : BETA - 1))
+    ntt_fwd_row_mac(RowMacArgs a, DeviceTables T) {
   extern __shared__ __align__(16) u64 rm_digits[];  // [regions][2 * WARPS rows][kRowPad]
   const int gid = PT ? a.mac.m + int(blockIdx.z) : int(blockIdx.z);
   if (T.tc[gid].q < kFreeModulusBound)

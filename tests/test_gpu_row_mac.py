@@ -113,3 +113,47 @@ def test_keyswitch_with_towers_at_the_reduction_free_bound(lib, orc, n):
             np.testing.assert_array_equal(nb.to_host(ob), wb, err_msg=f"L={level} rot={rot}")
             np.testing.assert_array_equal(nb.to_host(oa), wa, err_msg=f"L={level} rot={rot}")
     g.close()
+
+
+@pytest.mark.parametrize("n,m,k,dnum,levels", [(65536, 24, 8, 3, (24, 16)), (8192, 9, 3, 3, (9, 5)),
+                                               (4096, 16, 4, 4, (16, 13))])
+def test_inverse_row_pass_inside_the_fused_kernel(lib, orc, n, m, k, dnum, levels):
+    """The fused kernel's P towers run the ModDown's inverse row pass before
+    they are stored (row_mac_inv_rows, 2 to 4 digits, one request per input):
+    key switches, relinearizations and rotations by steps +-1 and +-64 (whole
+    rows gathered through the automorphism) equal the form with a separate
+    inverse row pass, and the oracle."""
+    ctx = synthetic_context(orc, n, m, k, dnum)
+    g = nb.Context.from_oracle(ctx)
+    keys = _keys(orc, ctx, 515)
+    five_inv = pow(5, -1, 2 * n)
+    autos = (5, five_inv, pow(5, 64, 2 * n), pow(five_inv, 64, 2 * n))
+    for level in levels:
+        cases = [Case(orc, ctx, level, 2000 + 10 * i + level, keys, "rotate", a) for i, a in enumerate(autos)]
+        cases.append(Case(orc, ctx, level, 2100 + level, keys, "switch"))
+        cases.append(Case(orc, ctx, level, 2200 + level, keys, "relin"))
+        got = {}
+        for fused in (1, 0):
+            nb.tuning_set("row_mac_inv_rows", fused)
+            try:
+                for c in cases:
+                    if c.kind == "relin":  # in place: restart from c0 / c1
+                        c.out_b.copy_(nb.to_device(c.c0))
+                        c.out_a.copy_(nb.to_device(c.c1))
+                reqs = [c.request() for c in cases]
+                g.keyswitch_requests(reqs, g.requests_workspace(reqs))
+                _sync()
+                got[fused] = [(nb.to_host(c.out_b), nb.to_host(c.out_a)) for c in cases]
+            finally:
+                nb.tuning_set("row_mac_inv_rows", 1)
+        for c, a, b in zip(cases, got[1], got[0]):
+            np.testing.assert_array_equal(a[0], b[0], err_msg=f"{c.kind} g={c.automorphism} L={level}")
+            np.testing.assert_array_equal(a[1], b[1], err_msg=f"{c.kind} g={c.automorphism} L={level}")
+        checked = cases if n <= 8192 else [cases[3], cases[5]]
+        for c in checked:
+            wb, wa = c.expected(orc, ctx)
+            i = cases.index(c)
+            np.testing.assert_array_equal(got[1][i][0], wb, err_msg=f"{c.kind} g={c.automorphism} L={level}")
+            np.testing.assert_array_equal(got[1][i][1], wa, err_msg=f"{c.kind} g={c.automorphism} L={level}")
+    assert g.device_errors() == 0
+    g.close()
