@@ -425,9 +425,11 @@ struct Timed {
     start = g_timer.take();
     CUDA_CHECK(cudaEventRecord(start, st));
   }
-  void done() {
+  // kernels: launches the record covers (the fused row pass + key
+  // multiplication is two: the Q towers, then the P towers).
+  void done(int kernels = 1) {
     CUDA_CHECK(cudaGetLastError());
-    g_launches += 1;
+    g_launches += kernels;
     if (!start) return;
     std::lock_guard<std::mutex> lock(g_timer.mu);
     cudaEvent_t stop = g_timer.take();
@@ -742,16 +744,32 @@ void launch_conv_t(const HostConvPlan &p, const b200::ConvArgs &a, dim3 grid, bo
   else
     b200::conv_kernel<MAXS, false, false><<<grid, b200::kEwThreads, 0, st>>>(a);
 }
-void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, const std::vector<uint16_t> &slots,
-                 size_t polys, u64 src_stride, u64 dst_stride, cudaStream_t st, bool lazy_out) {
+// One conversion of a tensor-core launch: plan, source and destination (the
+// polynomial strides are shared by the launch) and the targets' slots.
+struct ConvPart {
+  const HostConvPlan *plan;
+  u64 *dst;
+  const u64 *src;
+  std::vector<uint16_t> slots;
+};
+// Parts of one launch convert the same numbers of sources and targets.
+void run_conv_tc(const Ctx &c, const std::vector<ConvPart> &parts, size_t polys, u64 src_stride, u64 dst_stride,
+                 cudaStream_t st, bool lazy_out) {
+  require(!parts.empty() && parts.size() <= (size_t)b200::kTcMaxParts, "conversion parts out of range");
+  const HostConvPlan &p = *parts[0].plan;
   b200::ConvTcArgs a{};
-  a.plan = p.device;
-  a.bmat = p.tc_b;
-  a.src = src;
-  a.dst = dst;
+  for (size_t i = 0; i < parts.size(); ++i) {
+    const HostConvPlan &q = *parts[i].plan;
+    require(q.s == p.s && q.t == p.t && q.tc_kpad == p.tc_kpad && q.tc_groups == p.tc_groups && q.tc_b,
+            "conversions of one launch differ in shape");
+    a.part[i].plan = q.device;
+    a.part[i].bmat = q.tc_b;
+    a.part[i].src = parts[i].src;
+    a.part[i].dst = parts[i].dst;
+    for (size_t j = 0; j < parts[i].slots.size(); ++j) a.part[i].slot[j] = parts[i].slots[j];
+  }
   a.src_poly_stride = src_stride;
   a.dst_poly_stride = dst_stride;
-  for (size_t i = 0; i < slots.size(); ++i) a.slot[i] = slots[i];
   a.logn = c.logn;
   a.kpad = p.tc_kpad;
   a.groups = p.tc_groups;
@@ -760,15 +778,16 @@ void run_conv_tc(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src, 
   const int smem = b200::kTcThreads * p.tc_kpad + p.tc_groups * b200::kTcGroupRows * p.tc_kpad +
                    p.s * b200::kTcThreads * (int)sizeof(u64);
   ensure_conv_tc_attributes(c.device);
+  const size_t units = polys * parts.size();
   auto launch = [&](auto kernel) {
     const size_t tiles = c.n / b200::kTcThreads;
     // The tuned tiles per CTA, halved while the grid would cover fewer than 4
     // CTAs per SM (small batches: one request's switch is only 512 tiles).
     size_t per_cta = (size_t)tuned("conv_tc_tiles");
     const size_t want = 4 * (size_t)device_sms(c.device);
-    while (per_cta > 1 && ((tiles + per_cta - 1) / per_cta) * polys < want) per_cta = (per_cta + 1) / 2;
+    while (per_cta > 1 && ((tiles + per_cta - 1) / per_cta) * units < want) per_cta = (per_cta + 1) / 2;
     a.tiles_per_cta = (int)per_cta;
-    const dim3 grid((unsigned)((tiles + per_cta - 1) / per_cta), 1, (unsigned)polys);
+    const dim3 grid((unsigned)((tiles + per_cta - 1) / per_cta), (unsigned)parts.size(), (unsigned)polys);
     Timed t("conv", st);
     kernel<<<grid, b200::kTcThreads, smem, st>>>(a);
     t.done();
@@ -795,7 +814,7 @@ void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
   lazy_out = lazy_out && c.mode >= 1 && c.logn >= 12;
   require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
   if (p.tc_b && tuned("conv_tc") != 0) {
-    run_conv_tc(c, p, dst, src, slots, polys, src_stride, dst_stride, st, lazy_out);
+    run_conv_tc(c, {ConvPart{&p, dst, src, slots}}, polys, src_stride, dst_stride, st, lazy_out);
     return;
   }
   b200::ConvArgs a{};
@@ -822,6 +841,33 @@ void run_conv(const Ctx &c, const HostConvPlan &p, u64 *dst, const u64 *src,
   else if (p.s <= 16) launch_conv_t<16>(p, a, grid, lazy_out, st);
   else launch_conv_t<40>(p, a, grid, lazy_out, st);
   t.done();
+}
+
+// Conversions of several parts over the same polynomials and strides:
+// tensor-core parts of one shape share launches (up to kTcMaxParts each), the
+// others run one by one.
+void run_convs(const Ctx &c, const std::vector<ConvPart> &parts, size_t polys, u64 src_stride, u64 dst_stride,
+               cudaStream_t st, bool lazy_out = false) {
+  require(polys >= 1 && polys <= 65535, "polynomial batch out of range");
+  const bool lazy_tc = lazy_out && c.mode >= 1 && c.logn >= 12;
+  std::vector<ConvPart> batch;
+  auto flush = [&] {
+    if (!batch.empty()) run_conv_tc(c, batch, polys, src_stride, dst_stride, st, lazy_tc);
+    batch.clear();
+  };
+  for (const ConvPart &part : parts) {
+    const HostConvPlan &p = *part.plan;
+    if (!p.tc_b || tuned("conv_tc") == 0) {
+      flush();
+      run_conv(c, p, part.dst, part.src, part.slots, polys, src_stride, dst_stride, st, lazy_out);
+      continue;
+    }
+    if (!batch.empty() && (batch[0].plan->s != p.s || batch[0].plan->t != p.t ||
+                           batch.size() == (size_t)b200::kTcMaxParts))
+      flush();
+    batch.push_back(part);
+  }
+  flush();
 }
 
 // ---- workspace carving -----------------------------------------------------------
@@ -909,6 +955,7 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
           unscaled);
   const auto all = qp_ids(c, L);
   std::vector<Slot> fwd;
+  std::vector<ConvPart> convs;  // the digits' conversions: one launch where their shapes agree
   size_t digit = 0;
   for (size_t first = 0; first < L; first += c.alpha, ++digit) {
     const size_t count = std::min(c.alpha, L - first);
@@ -924,9 +971,10 @@ void do_digits(Ctx &c, size_t L, size_t polys, u64 *digits, const u64 *src, Carv
         slots.push_back((uint16_t)t);
         fwd.push_back({(uint32_t)(digit * T + t), all[t]});
       }
-    const auto &plan = c.conv_plan(range_ids(first, first + count), tgt, unscaled);
-    run_conv(c, plan, out, coeff + first * n, slots, polys, L * n, dstride, st, true);
+    convs.push_back({&c.conv_plan(range_ids(first, first + count), tgt, unscaled), out, coeff + first * n,
+                     std::move(slots)});
   }
+  run_convs(c, convs, polys, L * n, dstride, st, true);
   run_ntt(c, digits, digits, fwd, polys, dstride, dstride, false, st, nullptr, nullptr, false, lazy_out && !col_only,
           col_only);
 }
@@ -1117,7 +1165,7 @@ void do_row_mac(Ctx &c, size_t L, size_t inputs, u64 *out_b, u64 *out_a, u64 out
   a.p_inverse_rows = p_inverse_rows;
   Timed t("row_mac", st);
   CUDA_CHECK(b200::row_mac_launch(a, c.tables, c.logn, (int)beta, rot.on, (unsigned)inputs, (unsigned)T, st));
-  t.done();
+  t.done(T > L ? 2 : 1);
 }
 
 void do_rotate(Ctx &c, size_t L, size_t polys, u64 *out_b, u64 *out_a, const u64 *ext_b, const u64 *ext_a,

@@ -176,6 +176,8 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 // or brought to [0, m). It is congruent to conv_kernel's output modulo m_t,
 // hence identical once canonical.
 //
+// Grid: (runs of tiles_per_cta coefficient tiles, part, polynomial), where a
+// part is one conversion (plan, source, destination) of the launch.
 // CTA = 128 threads = 128 coefficients = the 128 TMEM lanes. A: one row of
 // 8s bytes per coefficient. B: groups of 8 targets (64 rows of 8s bytes),
 // built on the host per plan. Both use the canonical K-major layout without
@@ -191,13 +193,19 @@ __global__ void __launch_bounds__(kEwThreads) conv_limb_kernel(ConvArgs a) {
 constexpr int kTcThreads = 128;
 constexpr int kTcGroupTargets = 8;
 constexpr int kTcGroupRows = 64;  // 8 targets x 8 output bytes
-struct ConvTcArgs {
+// Conversions of one launch (grid y): the Hybrid digits of one level, which
+// all convert alpha sources into the L + K - alpha others, share one launch.
+constexpr int kTcMaxParts = 4;
+struct ConvTcPart {
   const ConvPlan *plan;
   const uint8_t *bmat;  // [groups][64 rows x kpad] bytes, canonical layout
   const u64 *src;
   u64 *dst;
-  u64 src_poly_stride, dst_poly_stride;
   uint16_t slot[kMaxConvTargets];
+};
+struct ConvTcArgs {
+  ConvTcPart part[kTcMaxParts];  // same source and target counts (and so kpad, groups) in every part
+  u64 src_poly_stride, dst_poly_stride;
   int logn, kpad, groups;
   int tiles_per_cta;  // coefficient tiles per CTA (B, TMEM and barriers set up once per CTA)
   int first_wait_polls;  // poll limit of the first bounded wait (for B); the others use kTcWaitPolls
@@ -255,14 +263,15 @@ __device__ __forceinline__ u64 tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo
 // constants (the plan must have exactly FS sources and FT targets), so the
 // per-tile loops unroll; zero takes them from the plan at run time.
 template <bool LAZY_OUT, int FS = 0, int FT = 0>
-__global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
+__global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(const __grid_constant__ ConvTcArgs a) {
   extern __shared__ __align__(1024) uint8_t tc_smem[];
   __shared__ __align__(8) u64 mbar, bbar;
   __shared__ uint32_t tmem_base;
   __shared__ u64 tm[kMaxConvTargets], twq[kMaxConvTargets];
   __shared__ u64 sq[kMaxConvSources];
   __shared__ Shoup sinv[kMaxConvSources];
-  const ConvPlan &p = *a.plan;
+  const ConvTcPart &part = a.part[blockIdx.y];
+  const ConvPlan &p = *part.plan;
   const int s = FS ? FS : p.s, t_count = FT ? FT : p.t;
   const int kpad = FS ? (8 * FS + 31) / 32 * 32 : a.kpad;
   const int groups = FT ? (FT + kTcGroupTargets - 1) / kTcGroupTargets : a.groups;
@@ -281,7 +290,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
             smem_addr(sb)),
-        "l"(a.bmat), "r"(bbytes), "r"(smem_addr(&bbar))
+        "l"(part.bmat), "r"(bbytes), "r"(smem_addr(&bbar))
         : "memory");
   }
   for (int t = tid; t < t_count; t += kTcThreads) {
@@ -300,8 +309,8 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
   __syncthreads();
   const uint32_t tmem = tmem_base;
   const u64 n = u64(1) << a.logn;
-  const u64 *src = a.src + blockIdx.z * a.src_poly_stride;
-  u64 *dst = a.dst + blockIdx.z * a.dst_poly_stride;
+  const u64 *src = part.src + blockIdx.z * a.src_poly_stride;
+  u64 *dst = part.dst + blockIdx.z * a.dst_poly_stride;
   // idesc: S32 accumulate, unsigned 8-bit A and B, K-major, N = 64, M = 128.
   const uint32_t idesc = (2u << 4) | (uint32_t(kTcGroupRows >> 3) << 17) | (uint32_t(kTcThreads >> 4) << 24);
   const uint32_t tiles = uint32_t(n / kTcThreads);
@@ -399,7 +408,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(ConvTcArgs a) {
           const u64 m = tm[t];
           u64 r = tc_fold_reduce(hi4, lo4, 0 - m, twq[t]);  // [0, 3.5m)
           if constexpr (!LAZY_OUT) r = csub_sign(csub_sign(r, 2 * m), m);
-          dst[u64(a.slot[t]) * n + k] = r;
+          dst[u64(part.slot[t]) * n + k] = r;
         }
       }
       // Every lane's loads are done before the next MMA reuses the columns.
