@@ -3,10 +3,10 @@
 Every tunable (ntt_b200_tuning_name) is a launch choice that never changes a
 result: the register budget each NTT pass is compiled for (3 or 4 resident
 CTAs per SM), whether the row passes stage their twiddles in shared memory, the
-conversion kernel (tensor cores, 30-bit limbs or 128-bit accumulators), the MAC
-kernel and
-the conversion grid target. The tuner runs coordinate descent over them on two
-workloads:
+conversion kernel (tensor cores, 30-bit limbs or 128-bit accumulators) and its
+tiles per CTA, the MAC kernel, and whether the key multiplication runs inside
+the digits' row pass (and the ModDown's inverse row pass inside that). The tuner
+runs coordinate descent over them on two workloads:
 
   * ntt:       forward + inverse NTT of 8 polynomials x 32 towers at N = 2^16
                (50/60-bit primes), one launch sequence per direction;
@@ -82,6 +82,9 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
     # while it is measured). The CUDA-core conversion choices serve the plans the tensor-core form
     # does not take (more than 16 sources, moduli outside [2^48, 2^61)), so they are measured with it off.
     cuda_core_conv = {"conv_tc": 0}
+    # The separate MAC's choices serve the key switches the fused row pass does not take (mode 0/1
+    # contexts, more than 4 digits), so they are measured with it off.
+    unfused_mac = {"row_mac": 0}
     plan = [
         ("ntt_minb_fwd_col", (3, 4), ntt_step, ("ntt_fwd_col",), {}),
         ("ntt_minb_fwd_row", (3, 4), ntt_step, ("ntt_fwd_row",), {}),
@@ -91,17 +94,17 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("ntt_row_direct", (0, 1), ntt_step, ("ntt_fwd_row", "ntt_inv_row"), {}),
         ("ntt_epi_stage", (0, 1), ks_step, ("ntt_fwd_row",), {}),
         ("intt_unscaled", (0, 1), ks_step, ("ntt_inv_col",), {}),
-        ("digits_lazy", (0, 1), ks_step, ("ntt_fwd_row", "mac"), {}),
+        ("digits_lazy", (0, 1), ks_step, ("ntt_fwd_row", "mac"), unfused_mac),
         ("ntt_stage_tw_fwd_row", (0, 1), ntt_step, ("ntt_fwd_row",), {}),
         ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",), {}),
         ("conv_limbs", (0, 1), ks_step, ("conv",), cuda_core_conv),
         ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",), cuda_core_conv),
-        ("mac_limbs", (0, 1), ks_step, ("mac",), {}),
-        ("mac_approx", (0, 1), ks_step, ("mac",), {"mac_limbs": 0}),
+        ("mac_limbs", (0, 1), ks_step, ("mac",), unfused_mac),
+        ("mac_approx", (0, 1), ks_step, ("mac",), {"mac_limbs": 0, **unfused_mac}),
         ("conv_tc", (0, 1), ks_step, ("conv",), {}),
         ("conv_tc_fixed", (0, 1), ks_step, ("conv",), {"conv_tc": 1}),
         ("conv_tc_tiles", (1, 2, 4, 8), ks_step, ("conv",), {"conv_tc": 1}),
-        ("row_mac", (0, 1), ks_step, ("ntt_fwd_row", "mac", "row_mac"), {}),
+        ("row_mac", (0, 1), ks_step, ("ntt_fwd_row", "mac", "row_mac", "ntt_inv_row"), {}),
         ("row_mac_inv_rows", (0, 1), ks_step, ("row_mac", "ntt_inv_row"), {"row_mac": 1}),
     ]
     measurements, choices = {}, {}
