@@ -59,3 +59,36 @@ def test_keyswitch_with_tensor_core_conversions(tc_on, orc, n, m, k, dnum):
     np.testing.assert_array_equal(nb.to_host(oa), wa)
     assert g.device_errors() == 0
     g.close()
+
+
+def test_conversion_run_lengths_give_identical_key_switches(tc_on, orc):
+    """One tensor-core launch converts all three Hybrid digits of 5 requests
+    (3 x 5 x 512 tiles of 128 coefficients). CTAs take runs of 4, 3 or 7
+    tiles; runs of 3 and 7 leave a short last run in every polynomial. Every
+    run length gives the same key switches, equal to the oracle."""
+    n, level, batch = 65536, 24, 5
+    ctx = synthetic_context(orc, n, level, 8, 3)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka = full_keys(orc, ctx, 19)
+    dkb, dka = nb.to_device(kb), nb.to_device(ka)
+    xs = np.stack([orc.lcg(n, ctx.q[:level], 40 + i) for i in range(batch)])
+    dx = nb.to_device(xs)
+    before = nb.tuning_get("conv_tc_tiles")
+    got = {}
+    try:
+        for tiles in (4, 3, 7):
+            nb.tuning_set("conv_tc_tiles", tiles)
+            ob, oa = nb.empty((batch, level, n)), nb.empty((batch, level, n))
+            g.keyswitch_batch(level, batch, ob, oa, dx, dkb, dka, g.workspace(nb.OP_KEYSWITCH, level, batch))
+            got[tiles] = (nb.to_host(ob), nb.to_host(oa))
+    finally:
+        nb.tuning_set("conv_tc_tiles", before)
+    assert g.device_errors() == 0
+    for tiles in (3, 7):
+        np.testing.assert_array_equal(got[tiles][0], got[4][0], err_msg=f"tiles={tiles}")
+        np.testing.assert_array_equal(got[tiles][1], got[4][1], err_msg=f"tiles={tiles}")
+    for i in (0, batch - 1):
+        wb, wa = orc.keyswitch(ctx, level, xs[i], kb, ka)
+        np.testing.assert_array_equal(got[4][0][i], wb)
+        np.testing.assert_array_equal(got[4][1][i], wa)
+    g.close()
