@@ -128,6 +128,50 @@ __device__ __forceinline__ Shoup tw_load(const ulonglong2 *p) {
   return Shoup{v.x, v.y};
 }
 
+// Gentleman-Sande stages that skip the sums' conditional subtraction (mode 2,
+// towers below 2^57): STAGES stages on 16 registers, register distances 1, 2,
+// 4, 8 in that order, registers entering below F * q. Each register's bound
+// after each stage is known at compile time (gs_bound): the sum of a pair
+// doubles the pair's bound, the difference side restarts below 4q (the
+// approximate-quotient product takes any word below 2^64), so the difference
+// is formed as x + bound(y) - y. From 4q the largest bound is 64q after four
+// stages, below 2^63. At the end every register takes exactly the conditional
+// subtractions that bring it below 4q: log2(bound / 4q) of them, 15 per thread
+// for four stages from 4q instead of one per butterfly (32).
+// tw_of(j, e): the Shoup twiddle of pair (e, e + 2^j) in stage j.
+__host__ __device__ constexpr int gs_bound(int f, int e, int j) {
+  int last = -1;  // the last stage (register bit) in which e was the difference side
+  for (int i = 0; i < j; ++i)
+    if ((e >> i) & 1) last = i;
+  return last < 0 ? f << j : 4 << (j - 1 - last);
+}
+template <int F, int STAGES, typename TwOf>
+__device__ __forceinline__ void gs_stages_light(u64 (&x)[16], TwOf tw_of, u64 q) {
+  const u64 qneg = 0 - q;
+#pragma unroll
+  for (int j = 0; j < STAGES; ++j) {
+    const int d = 1 << j;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_of(j, e);
+      const u64 s = x[e] + x[e + d];
+      x[e + d] = shoup_approx(x[e] + u64(gs_bound(F, e, j)) * q - x[e + d], w.w, w.wq, qneg);
+      x[e] = s;
+    }
+  }
+  static_assert(F <= 4 && STAGES <= 4, "bounds stay at or below 64q");
+  const u64 q4 = 4 * q, q8 = 8 * q, q16 = 16 * q, q32 = 32 * q;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int f = gs_bound(F, e, STAGES);  // x[e] < f q; each step halves the bound
+    if (f > 32) x[e] = csub_sign(x[e], q32);
+    if (f > 16) x[e] = csub_sign(x[e], q16);
+    if (f > 8) x[e] = csub_sign(x[e], q8);
+    if (f > 4) x[e] = csub_sign(x[e], q4);
+  }
+}
+
 // Coalesced copy of a [rows x width] global block (row stride `stride` words)
 // into shared memory with the given padded row pitch. width is a multiple of 2.
 template <int ROWS, int WIDTH, int PITCH, bool PAD16>
@@ -275,17 +319,14 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_col(NttBatch b, Dev
     fwd_col_body<LOGN, MODE, DIRECT, false>(b, T, tile, tw);
 }
 
-// UNSCALED: the last stage is a plain Gentleman-Sande butterfly (no N^-1) and
-// the outputs stay lazily reduced: N times the coefficients, in [0, 4q) for
-// mode 2 and [0, 2q) for mode 1. For a basis switch that folds N^-1 into its
-// constants (conv_plan with ninv), which reduces its inputs itself.
-template <int LOGN, int MODE, int MINB, bool DIRECT, bool UNSCALED = false>
-__global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
+// LIGHT (mode 2, q < 2^57): the stages before the last skip the sums'
+// reduction (gs_stages_light; each register phase ends below 4q), and the
+// last stage, with or without N^-1, runs as usual.
+template <int LOGN, int MODE, bool DIRECT, bool UNSCALED, bool LIGHT>
+__device__ __forceinline__ void inv_col_body(const NttBatch &b, const DeviceTables &T, u64 *tile, ulonglong2 *tw) {
   using G = ColGeom<LOGN>;
   constexpr int N = 1 << LOGN;
   constexpr u64 kStride = N >> G::LR;
-  __shared__ __align__(16) u64 tile[kTileWords];
-  __shared__ ulonglong2 tw[G::R];
   const TowerView v = tower_view(b, T, true);
   const u64 q = v.c->q, q2 = v.c->q2;
   const int col0 = blockIdx.x * G::COLS;
@@ -305,14 +346,25 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
       for (int e = 0; e < 16; ++e) x[e] = tile[G::row_b(e, u) * G::COLS + c];
     }
     // Stages logR-1 .. 4: row bit logR-1-s == register bit logR-1-s.
+    if constexpr (LIGHT) {
+      gs_stages_light<4, G::LR - 4>(
+          x,
+          [&](int j, int e) {
+            const int s = G::LR - 1 - j;
+            const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+            return Shoup{w.x, w.y};
+          },
+          q);
+    } else {
 #pragma unroll
-    for (int s = G::LR - 1; s >= 4; --s) {
-      const int d = 1 << (G::LR - 1 - s);
+      for (int s = G::LR - 1; s >= 4; --s) {
+        const int d = 1 << (G::LR - 1 - s);
 #pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        if (e & d) continue;
-        const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
-        gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+        for (int e = 0; e < 16; ++e) {
+          if (e & d) continue;
+          const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+          gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+        }
       }
     }
     if constexpr (!DIRECT) __syncthreads();  // every thread has read its inputs from the tile
@@ -326,14 +378,25 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
     for (int e = 0; e < 16; ++e) x[e] = tile[G::row_a(e, u) * G::COLS + c];
   }
   // Stages 3..1, then stage 0 with N^-1 folded in.
+  if constexpr (LIGHT) {
+    gs_stages_light<4, 3>(
+        x,
+        [&](int j, int e) {
+          const int s = 3 - j;
+          const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
+          return Shoup{w.x, w.y};
+        },
+        q);
+  } else {
 #pragma unroll
-  for (int s = 3; s >= 1; --s) {
-    const int d = 8 >> s;
+    for (int s = 3; s >= 1; --s) {
+      const int d = 8 >> s;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      if (e & d) continue;
-      const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
-      gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const ulonglong2 w = tw[(1 << s) + (e >> (4 - s))];
+        gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+      }
     }
   }
   if constexpr (UNSCALED) {
@@ -356,6 +419,21 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, Dev
   for (int e = 0; e < 16; ++e) tile[G::row_a(e, u) * G::COLS + c] = x[e];
   __syncthreads();
   store_block<G::R, G::COLS, G::COLS, false>(tower_dst(b, T, fresh_block_ids()) + col0, tile, kStride);
+}
+
+// UNSCALED: the last stage is a plain Gentleman-Sande butterfly (no N^-1) and
+// the outputs stay lazily reduced: N times the coefficients, in [0, 4q) for
+// mode 2 and [0, 2q) for mode 1. For a basis switch that folds N^-1 into its
+// constants (conv_plan with ninv), which reduces its inputs itself.
+// The CTA's tower decides the butterflies: reduction-light below 2^57 (mode 2).
+template <int LOGN, int MODE, int MINB, bool DIRECT, bool UNSCALED = false>
+__global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_col(NttBatch b, DeviceTables T) {
+  __shared__ __align__(16) u64 tile[kTileWords];
+  __shared__ ulonglong2 tw[ColGeom<LOGN>::R];
+  if (MODE == 2 && T.tc[b.id[blockIdx.z]].q < kFreeModulusBound)
+    inv_col_body<LOGN, MODE, DIRECT, UNSCALED, MODE == 2>(b, T, tile, tw);
+  else
+    inv_col_body<LOGN, MODE, DIRECT, UNSCALED, false>(b, T, tile, tw);
 }
 
 // ---- row pass ----------------------------------------------------------------
@@ -610,39 +688,66 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
 // word e*16 + u. `my` is the row's padded shared-memory buffer, used for the
 // exchange between the two register phases; the row's threads may still be
 // reading it on entry (the exchange starts with __syncwarp).
-template <int LOGN, int MODE>
+// LIGHT (mode 2, q < 2^57): the stages skip the sums' reduction
+// (gs_stages_light); either way the outputs lie below 4q.
+template <int LOGN, int MODE, bool LIGHT = false>
 __device__ __forceinline__ void inv_row_stages(u64 (&x)[16], u64 *my, const ulonglong2 *tw, int row, int u, u64 q,
                                                u64 q2) {
   constexpr int LR = LOGN - 8;
-  // Stages LR + s', s' = 7..4: column bit 7-s' == register bit 7-s'.
+  if constexpr (LIGHT) {
+    static_assert(MODE == 2, "reduction-light butterflies are mode 2");
+    // Stages LR + 7 - j, j = 0..3, then LR + 3 - j: canonical inputs (F = 1).
+    gs_stages_light<1, 4>(
+        x,
+        [&](int j, int e) {
+          const int sp = 7 - j;
+          return tw_load(tw + (1 << (LR + sp)) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
+        },
+        q);
+    __syncwarp();
 #pragma unroll
-  for (int sp = 7; sp >= 4; --sp) {
-    const int s = LR + sp, d = 1 << (7 - sp);
+    for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
+    __syncwarp();
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      if (e & d) continue;
-      const Shoup w = tw_load(tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
-      if (sp == 7)
-        gs_butterfly<MODE, true>(x[e], x[e + d], w.w, w.wq, q, q2);
-      else
-        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+    for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+    gs_stages_light<4, 4>(
+        x,
+        [&](int j, int e) {
+          const int sp = 3 - j;
+          return tw_load(tw + (1 << (LR + sp)) + (row << sp) + (e >> (4 - sp)));
+        },
+        q);
+  } else {
+    // Stages LR + s', s' = 7..4: column bit 7-s' == register bit 7-s'.
+#pragma unroll
+    for (int sp = 7; sp >= 4; --sp) {
+      const int s = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const Shoup w = tw_load(tw + (1 << s) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
+        if (sp == 7)
+          gs_butterfly<MODE, true>(x[e], x[e + d], w.w, w.wq, q, q2);
+        else
+          gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
     }
-  }
-  __syncwarp();
+    __syncwarp();
 #pragma unroll
-  for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
-  __syncwarp();
+    for (int e = 0; e < 16; ++e) my[pad_col(u * 16 + e)] = x[e];
+    __syncwarp();
 #pragma unroll
-  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
-  // Stages LR + s', s' = 3..0: column bit 7-s' == register bit 3-s'.
+    for (int e = 0; e < 16; ++e) x[e] = my[pad_col(e * 16 + u)];
+    // Stages LR + s', s' = 3..0: column bit 7-s' == register bit 3-s'.
 #pragma unroll
-  for (int sp = 3; sp >= 0; --sp) {
-    const int s = LR + sp, d = 8 >> sp;
+    for (int sp = 3; sp >= 0; --sp) {
+      const int s = LR + sp, d = 8 >> sp;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      if (e & d) continue;
-      const Shoup w = tw_load(tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
-      gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const Shoup w = tw_load(tw + (1 << s) + (row << sp) + (e >> (4 - sp)));
+        gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+      }
     }
   }
 }
@@ -701,6 +806,8 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_inv_row(NttBatch b, Dev
         gs_butterfly<MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
       }
     }
+  } else if (MODE == 2 && q < kFreeModulusBound) {
+    inv_row_stages<LOGN, MODE, MODE == 2>(x, my, v.tw, row, u, q, q2);
   } else {
     inv_row_stages<LOGN, MODE>(x, my, v.tw, row, u, q, q2);
   }

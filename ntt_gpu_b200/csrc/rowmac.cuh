@@ -287,7 +287,7 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
               ROT ? __brev((base + 16 * ((kBr4[e] * g16) & 15u)) & 255u) >> 24 : uint32_t(u * 16 + e);
           x[e] = my[pad_col(int(cs))];
         }
-        inv_row_stages<LOGN, 2>(x, my, itw, rd, u, q, q2);
+        inv_row_stages<LOGN, 2, FREE>(x, my, itw, rd, u, q, q2);
         u64 *o = (ch == 0 ? a.mac.out_b : a.mac.out_a) + obase + u64(rd) * 256 + u;
 #pragma unroll
         for (int e = 0; e < 16; ++e) o[e * 16] = x[e];

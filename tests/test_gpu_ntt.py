@@ -106,13 +106,15 @@ def primes_below(orc, n, count, bound):
 
 
 @pytest.mark.parametrize("bits", [[61], [62], [61, 62], [59, 61], [-57], [58], [-57, 58], [30, 45, -57]])
-@pytest.mark.parametrize("logn", [12, 16])
+@pytest.mark.parametrize("logn", [12, 14, 16])
 def test_butterfly_mode_boundaries(lib, orc, bits, logn):
     """Moduli just below 2^61 (fast approximate-quotient butterflies, values up to
     8q), in [2^61, 2^62) (Harvey lazy butterflies), just below 2^57 (forward
-    butterflies without per-stage reductions, values up to 68q) and just above
-    it, and mixed within one launch: exact results, with all-(q-1) inputs
-    driving every stage to the top of its range."""
+    butterflies without per-stage reductions, values up to 68q; inverse
+    butterflies without the sums' reduction, up to 64q within a register phase)
+    and just above it, and mixed within one launch: exact results, with
+    all-(q-1) inputs driving every stage to the top of its range. logN = 14
+    leaves the inverse column pass a first register phase of two stages."""
     n = 1 << logn
     q = []
     for b in bits:  # b < 0: the primes just below 2^|b|
