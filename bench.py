@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "keyswitch/s N=2^16 L=24 dnum=3 served vs plain, p50/p99 ms; NTT HBM GB/s"
 UNIT = "keyswitch/s"
 N, LEVEL, K_P, DNUM, BATCH = 65536, 24, 8, 3, 16
-E2E_CHUNK = 1  # requests per chunk of the host-buffer pipeline (best of 1, 2, 4, 8, 16 on a B200)
+E2E_CHUNK = 4  # requests per chunk of the host-buffer pipeline (best of 1, 2, 4 with back-to-back asynchronous calls on a B200)
 SEED = 0x7251D9
 WORKLOAD = ("batched Hybrid key switch: 16 ciphertext components per GPU at N=2^16, L=24 (55-bit), "
             "K=8 (60-bit), dnum=3 (alpha=8), one shared switching key")
@@ -54,6 +54,8 @@ def parse():
                     help="profiling: override a launch tunable (repeatable), e.g. --tune conv_tc=0")
     ap.add_argument("--rotate", action="store_true",
                     help="profiling: every batched request also adds P*c0 and rotates by g = 5 (rotate kernel)")
+    ap.add_argument("--e2e-chunk", type=int, default=E2E_CHUNK,
+                    help="requests per chunk of the end-to-end host-buffer pipeline")
     ap.add_argument("--kernels-only", action="store_true",
                     help="timed batched steps only (no plain/e2e/CPU legs); for profiler launch lists")
     return ap.parse_args()
@@ -767,37 +769,47 @@ def run_ours(args, rank, world, local):
              "note": "same kernels, one request per call, back to back on one stream"}
 
     # ---- end to end through the public API with host buffers -----------------------------------------
-    # ntt_b200_keyswitch_host: pinned host inputs and outputs; the batch runs in chunks whose copies to
-    # and from the device overlap each other and the kernels. The timed region holds every step's
-    # host->device copy of its inputs and device->host copy of both outputs.
+    # ntt_b200_keyswitch_host_async: pinned host inputs and outputs; each step's batch runs in chunks whose
+    # copies to and from the device overlap each other and the kernels, and the next step starts while the
+    # last outputs are still leaving; ntt_b200_keyswitch_host_wait joins the caller's stream at the end of
+    # the timed region. The timed region holds every step's host->device copy of its inputs and
+    # device->host copy of both outputs. The synchronous form (the stream waits for each step's outputs)
+    # is timed the same way and reported beside it.
     h_x = torch.from_numpy(x.view("int64")).pin_memory()
     h_b = torch.empty((B, LEVEL, N), dtype=torch.int64).pin_memory()
     h_a = torch.empty_like(h_b).pin_memory()
     e2e_steps = max(3, min(args.steps, 10))
-    chunk = E2E_CHUNK
+    chunk = args.e2e_chunk
     ws_host = ctx.host_workspace(LEVEL, chunk)
 
-    def e2e_step():
-        ctx.keyswitch_host(LEVEL, B, chunk, h_x, h_b, h_a, d_kb, d_ka, ws_host, stream=stream)
+    def e2e_run(steps, wait):
+        for _ in range(steps):
+            ctx.keyswitch_host(LEVEL, B, chunk, h_x, h_b, h_a, d_kb, d_ka, ws_host, stream=stream, wait=wait)
+        ctx.keyswitch_host_wait(stream)
 
-    for _ in range(3):
-        e2e_step()
-    barrier(world)
-    torch.cuda.synchronize(dev)
-    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    q0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    q1.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = max_over_ranks(q0.elapsed_time(q1), world, dev)
+    def e2e_time(wait):
+        e2e_run(3, wait)
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        e2e_run(e2e_steps, wait)
+        q1.record(stream)
+        torch.cuda.synchronize(dev)
+        return max_over_ranks(q0.elapsed_time(q1), world, dev)
+
+    e2e_sync_ms = e2e_time(True)
+    e2e_ms = e2e_time(False)
     ref_b = torch.empty_like(out_b)
     ctx.keyswitch_batch(LEVEL, B, ref_b, out_a, d_x, d_kb, d_ka, ws, stream=stream)
     torch.cuda.synchronize(dev)
     e2e_exact = bool(torch.equal(ref_b.cpu(), h_b))
     e2e = {"value": B * e2e_steps * world / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(h_x.numel() * 8), "d2h_bytes_per_step": int((h_b.numel() + h_a.numel()) * 8),
-           "steps": e2e_steps, "api": f"ntt_b200_keyswitch_host, pinned host buffers, chunks of {chunk}",
+           "steps": e2e_steps,
+           "api": f"ntt_b200_keyswitch_host_async per step + ntt_b200_keyswitch_host_wait, pinned host buffers, "
+                  f"chunks of {chunk}",
+           "synchronous_value": B * e2e_steps * world / (e2e_sync_ms / 1000.0),
            "outputs_equal_device_path": e2e_exact}
     # The copy bound of that number: the same step's bytes moved by plain pinned copies alone, the outputs
     # device-to-host while the inputs go host-to-device on another stream (no kernels).

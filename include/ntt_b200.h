@@ -327,6 +327,18 @@ int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, si
                             const uint64_t *h_src, uint64_t *h_out_b, uint64_t *h_out_a,
                             const uint64_t *key_b, const uint64_t *key_a, const uint64_t *h_c0,
                             uint32_t automorphism, void *workspace, size_t workspace_bytes, void *stream);
+/* The same key switch without the final wait: `stream` does not wait for the
+ * copies of the outputs to the host, so the next host-buffer call on this
+ * context (same workspace) starts copying and switching while this call's last
+ * outputs are still leaving, and back-to-back calls keep both copy directions
+ * busy. The two staging slots stay ordered across calls. The outputs of every
+ * call so far are on the host once ntt_b200_keyswitch_host_wait has made a
+ * stream wait for them and that stream has reached that point. */
+int ntt_b200_keyswitch_host_async(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk,
+                                  const uint64_t *h_src, uint64_t *h_out_b, uint64_t *h_out_a,
+                                  const uint64_t *key_b, const uint64_t *key_a, const uint64_t *h_c0,
+                                  uint32_t automorphism, void *workspace, size_t workspace_bytes, void *stream);
+int ntt_b200_keyswitch_host_wait(ntt_b200_context ctx, void *stream);
 
 /* MAC with per-digit device pointers (count digits of L+K towers each):
  * full_key_rows != 0 -> key pointers are full-context digits (rows chosen by

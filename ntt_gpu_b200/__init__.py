@@ -68,6 +68,8 @@ _SIGNATURES = {
     "ntt_b200_keyswitch_requests": ([_P, _P, _SZ, _P, _SZ, _P], _I),
     "ntt_b200_keyswitch_host_workspace": ([_P, _SZ, _SZ, _I, ctypes.POINTER(_SZ)], _I),
     "ntt_b200_keyswitch_host": ([_P, _SZ, _SZ, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
+    "ntt_b200_keyswitch_host_async": ([_P, _SZ, _SZ, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _SZ, _P], _I),
+    "ntt_b200_keyswitch_host_wait": ([_P, _P], _I),
     "ntt_b200_server_last_error": ([], ctypes.c_char_p),
     "ntt_b200_server_create": ([ctypes.POINTER(_P), _P], _I),
     "ntt_b200_server_submit": ([_P, _P, _P, ctypes.POINTER(_U64)], _I),
@@ -392,16 +394,21 @@ class Context:
         return torch.empty(max(1, (out.value + 7) // 8), dtype=torch.int64, device=f"cuda:{self.device}")
 
     def keyswitch_host(self, level, batch, chunk, h_src, h_out_b, h_out_a, key_b, key_a, workspace, h_c0=None,
-                       automorphism=0, stream=None):
-        """Host tensors (pinned CPU int64) in and out; keys and workspace on the device."""
+                       automorphism=0, stream=None, wait=True):
+        """Host tensors (pinned CPU int64) in and out; keys and workspace on the device.
+        wait=False: ntt_b200_keyswitch_host_async (join later with keyswitch_host_wait)."""
         def hp(t):
             if t is None:
                 return None
             assert not t.is_cuda and t.is_contiguous()
             return t.data_ptr()
-        _check(self._lib.ntt_b200_keyswitch_host(self._h, level, batch, chunk, hp(h_src), hp(h_out_b), hp(h_out_a),
-                                                 _ptr(key_b), _ptr(key_a), hp(h_c0), automorphism, _ptr(workspace),
-                                                 workspace.numel() * 8, _stream(stream)))
+        fn = self._lib.ntt_b200_keyswitch_host if wait else self._lib.ntt_b200_keyswitch_host_async
+        _check(fn(self._h, level, batch, chunk, hp(h_src), hp(h_out_b), hp(h_out_a), _ptr(key_b), _ptr(key_a),
+                  hp(h_c0), automorphism, _ptr(workspace), workspace.numel() * 8, _stream(stream)))
+
+    def keyswitch_host_wait(self, stream=None):
+        """Make `stream` wait for the outputs of every host-buffer key switch so far."""
+        _check(self._lib.ntt_b200_keyswitch_host_wait(self._h, _stream(stream)))
 
     def host_transform_workspace(self, op):
         import torch

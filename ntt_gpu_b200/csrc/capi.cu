@@ -2059,10 +2059,14 @@ int ntt_b200_keyswitch_host_workspace(ntt_b200_context ctx, size_t level, size_t
   });
 }
 
-int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk, const uint64_t *h_src,
-                            uint64_t *h_out_b, uint64_t *h_out_a, const uint64_t *key_b, const uint64_t *key_a,
-                            const uint64_t *h_c0, uint32_t automorphism, void *workspace, size_t ws_size,
-                            void *stream) {
+namespace {
+// The host-buffer pipeline; `join` makes the caller's stream wait for the
+// outputs' copies at the end (ntt_b200_keyswitch_host), else the caller joins
+// later (ntt_b200_keyswitch_host_async + ntt_b200_keyswitch_host_wait).
+int keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk, const uint64_t *h_src,
+                   uint64_t *h_out_b, uint64_t *h_out_a, const uint64_t *key_b, const uint64_t *key_a,
+                   const uint64_t *h_c0, uint32_t automorphism, void *workspace, size_t ws_size, void *stream,
+                   bool join) {
   return guarded([&] {
     require_ctx(ctx);
     require_level(ctx, level);
@@ -2119,6 +2123,40 @@ int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, si
       CUDA_CHECK(cudaEventRecord(c.ev_out[sl], c.copy_out));
     }
     // The caller's stream continues once every output has reached the host.
+    if (join) {
+      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[0], 0));
+      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[1], 0));
+    }
+  });
+}
+}  // namespace
+
+int ntt_b200_keyswitch_host(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk, const uint64_t *h_src,
+                            uint64_t *h_out_b, uint64_t *h_out_a, const uint64_t *key_b, const uint64_t *key_a,
+                            const uint64_t *h_c0, uint32_t automorphism, void *workspace, size_t ws_size,
+                            void *stream) {
+  return keyswitch_host(ctx, level, batch, chunk, h_src, h_out_b, h_out_a, key_b, key_a, h_c0, automorphism,
+                        workspace, ws_size, stream, true);
+}
+
+int ntt_b200_keyswitch_host_async(ntt_b200_context ctx, size_t level, size_t batch, size_t chunk,
+                                  const uint64_t *h_src, uint64_t *h_out_b, uint64_t *h_out_a,
+                                  const uint64_t *key_b, const uint64_t *key_a, const uint64_t *h_c0,
+                                  uint32_t automorphism, void *workspace, size_t ws_size, void *stream) {
+  return keyswitch_host(ctx, level, batch, chunk, h_src, h_out_b, h_out_a, key_b, key_a, h_c0, automorphism,
+                        workspace, ws_size, stream, false);
+}
+
+int ntt_b200_keyswitch_host_wait(ntt_b200_context ctx, void *stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    Ctx &c = *ctx;
+    DeviceGuard guard(c.device);
+    std::lock_guard<std::mutex> lock(c.pipe_mu);
+    if (!c.copy_in) return;  // no host-buffer call has run on this context
+    // The copies to the host run in order on one stream, so its latest two
+    // records (one per staging slot) cover every earlier one.
+    const cudaStream_t st = as_stream(stream);
     CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[0], 0));
     CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[1], 0));
   });

@@ -199,3 +199,35 @@ def test_host_buffer_pipeline_matches_oracle(lib, orc, batch, chunk, rotate):
             np.testing.assert_array_equal(h_b[r].numpy().view(np.uint64), wb)
             np.testing.assert_array_equal(h_a[r].numpy().view(np.uint64), wa)
     g.close()
+
+
+def test_async_host_calls_back_to_back(lib, orc):
+    """ntt_b200_keyswitch_host_async: four calls in a row on one stream with no
+    wait between them (batch 5 in chunks of 2, so the calls start on either
+    staging slot), the last one writing into the first one's host buffers;
+    ntt_b200_keyswitch_host_wait then joins the stream. Synchronising that
+    stream alone makes every output visible, each equal to the oracle."""
+    import torch
+    ctx = synthetic_context(orc, 8192, 6, 3, 2)
+    g = nb.Context.from_oracle(ctx)
+    kb, ka, dkb, dka = _keys(orc, ctx, 63)
+    level, batch, chunk = 5, 5, 2
+    ws = g.host_workspace(level, chunk)
+    stream = torch.cuda.current_stream()
+    xs = [np.stack([orc.lcg(ctx.n, ctx.q[:level], 700 + 10 * call + r) for r in range(batch)]) for call in range(4)]
+    h_x = [torch.from_numpy(x.view(np.int64)).pin_memory() for x in xs]
+    h_out = [(torch.zeros(xs[0].shape, dtype=torch.int64).pin_memory(),
+              torch.zeros(xs[0].shape, dtype=torch.int64).pin_memory()) for _ in range(3)]
+    torch.cuda.synchronize()
+    for call in range(4):
+        h_b, h_a = h_out[call % 3]
+        g.keyswitch_host(level, batch, chunk, h_x[call], h_b, h_a, dkb, dka, ws, stream=stream, wait=False)
+    g.keyswitch_host_wait(stream)
+    stream.synchronize()
+    for buf, call in ((0, 3), (1, 1), (2, 2)):
+        h_b, h_a = h_out[buf]
+        for r in range(batch):
+            wb, wa = orc.keyswitch(ctx, level, xs[call][r], kb, ka)
+            np.testing.assert_array_equal(h_b[r].numpy().view(np.uint64), wb, err_msg=f"call {call}")
+            np.testing.assert_array_equal(h_a[r].numpy().view(np.uint64), wa, err_msg=f"call {call}")
+    g.close()
