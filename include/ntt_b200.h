@@ -20,7 +20,9 @@
  *    enqueued; callers synchronise on the stream.
  *  - Every call validates its arguments on the host and returns a contract
  *    error BEFORE anything is enqueued (reference: ContractError thrown before
- *    enqueue, include/ntt/backend_contract.hpp:20-26).
+ *    enqueue, include/ntt/backend_contract.hpp:20-26). The host-array
+ *    transforms check the arrays' contents while copying them in and compute
+ *    nothing before every word has passed (see ntt_b200_host_transform).
  *  - Scratch: composite operations take a caller-provided device workspace whose
  *    size ntt_b200_workspace_bytes reports; they never allocate.
  */
@@ -412,14 +414,18 @@ int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, 
  *   POINTWISE: values *= right (both evaluation form);
  *   MULTIPLY: values = the ring product of values and right mod x^N + 1
  *     (coefficient form in and out).
- * Every residue is checked against its tower's modulus on the host before
- * anything is enqueued (the reference's validate_values; a contract error
- * otherwise). The call is synchronous, like the reference's: it returns once
- * the results are back in host memory. The towers move in chunks of 4 through
- * two device staging slots in `workspace` (ntt_b200_host_transform_workspace
- * bytes), on the context's copy streams, so host->device copies, transforms
- * and device->host copies of different chunks overlap (with pinned host memory;
- * pageable memory works, with less overlap). */
+ * Every residue is checked against its tower's modulus on the host before any
+ * result is computed or written (the reference's validate_values; a contract
+ * error otherwise): the calling thread checks the towers in chunks and each
+ * checked chunk is copied to the device while the next one is checked; the
+ * transforms and the copies back to the host run once every residue has
+ * passed. On a failed check the call waits for the copies it has started and
+ * returns the contract error with `values` unchanged. The call is synchronous,
+ * like the reference's: it returns once the results are back in host memory.
+ * `workspace` holds every tower of the call, once per operand:
+ * ntt_b200_host_transform_workspace reports that size for the context's own
+ * towers (a call that repeats tower ids needs more). Host memory should be
+ * pinned for the copies to overlap the checks; pageable memory works. */
 #define NTT_B200_HOST_FORWARD 0
 #define NTT_B200_HOST_INVERSE 1
 #define NTT_B200_HOST_POINTWISE 2

@@ -488,6 +488,7 @@ Tunable g_tuning[] = {
     {"row_mac", {1}, 0, 1},            // key multiplication fused into the digits' forward row pass
     {"row_mac_max_beta", {4}, 1, 4},   // largest digit count the fused row pass takes (shared memory per CTA grows with it)
     {"row_mac_inv_rows", {1}, 0, 1},   // its P towers run the ModDown's inverse row pass before they are stored
+    {"host_chunk_towers", {4}, 1, 128}, // towers the host-array transforms check and copy per step
 };
 Tunable *find_tunable(const char *name) {
   for (auto &t : g_tuning)
@@ -2337,41 +2338,31 @@ int ntt_b200_mod_down_static(ntt_b200_context ctx, size_t level, uint64_t *dst, 
 
 // ---- host-buffer transforms (the reference's CudaNttTransform public calls) ---------------
 namespace {
-constexpr size_t kHostChunkTowers = 4;  // towers per staging slot and operand
+// Towers the host-array transforms check and copy per step (tunable
+// host_chunk_towers): a checked chunk is copied while the next is checked.
+size_t host_chunk_towers() { return (size_t)tuned("host_chunk_towers"); }
 
-size_t host_transform_slot_words(const Ctx &c, int op) {
-  return (op >= NTT_B200_HOST_POINTWISE ? 2 : 1) * kHostChunkTowers * c.n;
+// Device words of a host-array transform's workspace: every tower of the
+// context, once per operand.
+size_t host_transform_words(const Ctx &c, int op) {
+  return (op >= NTT_B200_HOST_POINTWISE ? 2 : 1) * c.towers() * c.n;
 }
 
-// Every residue below its tower's modulus (the reference's validate_values),
-// on the host before anything is enqueued; large inputs are split over threads.
-// With q < 2^63, x < q exactly when neither x nor (q - 1 - x) mod 2^64 has its
-// top bit set, so the scan is a subtraction and two ORs per word, which the
-// compiler vectorises.
-void validate_host_values(const Ctx &c, const u64 *v, const std::vector<uint16_t> &ids) {
-  const size_t n = c.n, towers = ids.size();
-  auto scan = [&](size_t t0, size_t t1) {
-    u64 flags = 0;
-    for (size_t t = t0; t < t1; ++t) {
-      const u64 qm1 = c.mod[ids[t]] - 1;
-      const u64 *p = v + t * n;
-      for (size_t i = 0; i < n; ++i) flags |= (qm1 - p[i]) | p[i];
-    }
-    return (flags >> 63) == 0;
-  };
-  const size_t threads = std::min<size_t>(towers, towers * n >= (size_t(1) << 20) ? 8 : 1);
-  bool ok = true;
-  if (threads <= 1) {
-    ok = scan(0, towers);
-  } else {
-    std::vector<std::thread> pool;
-    std::vector<char> part(threads, 1);
-    for (size_t w = 0; w < threads; ++w)
-      pool.emplace_back([&, w] { part[w] = scan(towers * w / threads, towers * (w + 1) / threads); });
-    for (auto &th : pool) th.join();
-    for (char r : part) ok = ok && r;
+// Whether towers [first, first + count) of a host array (its tower i at
+// v + i * N) are canonical residues of their moduli (the reference's
+// validate_values). With q < 2^63, x < q exactly when neither x nor
+// (q - 1 - x) mod 2^64 has its top bit set, so one OR over the towers decides
+// it without a branch per word.
+bool host_values_canonical(const Ctx &c, const u64 *v, const std::vector<uint16_t> &ids, size_t first,
+                           size_t count) {
+  const size_t n = c.n;
+  u64 flags = 0;
+  for (size_t t = first; t < first + count; ++t) {
+    const u64 qm1 = c.mod[ids[t]] - 1;
+    const u64 *p = v + t * n;
+    for (size_t i = 0; i < n; ++i) flags |= (qm1 - p[i]) | p[i];
   }
-  require(ok, "host values must be canonical residues of their towers");
+  return (flags >> 63) == 0;
 }
 
 void launch_pointwise(const Ctx &c, u64 *dst, const u64 *left, const u64 *right, const std::vector<Slot> &slots,
@@ -2397,7 +2388,7 @@ int ntt_b200_host_transform_workspace(ntt_b200_context ctx, int op, size_t *byte
     require_ctx(ctx);
     require(bytes != nullptr && op >= NTT_B200_HOST_FORWARD && op <= NTT_B200_HOST_MULTIPLY,
             "invalid host transform query");
-    *bytes = 2 * aligned_bytes(host_transform_slot_words(*ctx, op));
+    *bytes = aligned_bytes(host_transform_words(*ctx, op));
   });
 }
 
@@ -2418,53 +2409,56 @@ int ntt_b200_host_transform(ntt_b200_context ctx, int op, uint64_t *values, cons
       ids[i] = (uint16_t)tower_ids[i];
     }
     require_aligned({workspace});
-    const size_t slot_words = host_transform_slot_words(c, op);
-    if (!workspace || ws_size < 2 * aligned_bytes(slot_words)) throw WorkspaceError("workspace missing or too small");
-    validate_host_values(c, values, ids);
-    if (two) validate_host_values(c, right, ids);
+    // Every tower of this call, once per operand (tower ids may repeat, so this
+    // can exceed the size the workspace query reports for the context).
+    if (!workspace || ws_size < aligned_bytes((two ? 2 : 1) * towers * c.n))
+      throw WorkspaceError("workspace missing or too small");
     DeviceGuard guard(c.device);
     std::lock_guard<std::mutex> lock(c.pipe_mu);
     ensure_copy_pipeline(c);
     const cudaStream_t st = as_stream(stream);
     const size_t n = c.n;
-    char *base = reinterpret_cast<char *>(workspace);
-    u64 *slot[2] = {reinterpret_cast<u64 *>(base), reinterpret_cast<u64 *>(base + aligned_bytes(slot_words))};
+    u64 *d_l = reinterpret_cast<u64 *>(workspace), *d_r = d_l + towers * n;
+    // The copies start after the work already on the caller's stream. Each
+    // chunk is checked on this thread and then copied while the next one is
+    // checked; nothing is computed or written back before every residue passed.
     CUDA_CHECK(cudaEventRecord(c.ev_start, st));
     CUDA_CHECK(cudaStreamWaitEvent(c.copy_in, c.ev_start, 0));
-    CUDA_CHECK(cudaStreamWaitEvent(c.copy_out, c.ev_start, 0));
-    for (size_t first = 0, k = 0; first < towers; first += kHostChunkTowers, ++k) {
-      const size_t r = std::min(kHostChunkTowers, towers - first);
-      const int sl = (int)(k & 1);
-      u64 *d_l = slot[sl], *d_r = d_l + kHostChunkTowers * n;
-      // host -> device, once the transforms two chunks back have read this slot
-      CUDA_CHECK(cudaStreamWaitEvent(c.copy_in, c.ev_comp[sl], 0));
-      CUDA_CHECK(cudaMemcpyAsync(d_l, values + first * n, r * n * sizeof(u64), cudaMemcpyHostToDevice, c.copy_in));
+    const size_t chunk = host_chunk_towers();
+    bool ok = true;
+    for (size_t first = 0; first < towers && ok; first += chunk) {
+      const size_t r = std::min(chunk, towers - first);
+      ok = host_values_canonical(c, values, ids, first, r) && (!two || host_values_canonical(c, right, ids, first, r));
+      if (!ok) break;
+      CUDA_CHECK(cudaMemcpyAsync(d_l + first * n, values + first * n, r * n * sizeof(u64), cudaMemcpyHostToDevice,
+                                 c.copy_in));
       if (two)
-        CUDA_CHECK(cudaMemcpyAsync(d_r, right + first * n, r * n * sizeof(u64), cudaMemcpyHostToDevice, c.copy_in));
-      CUDA_CHECK(cudaEventRecord(c.ev_in[sl], c.copy_in));
-      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_in[sl], 0));
-      CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[sl], 0));
-      std::vector<Slot> slots;
-      for (size_t i = 0; i < r; ++i) slots.push_back({(uint32_t)i, ids[first + i]});
-      const u64 stride = r * n;
-      switch (op) {
-        case NTT_B200_HOST_FORWARD: run_ntt(c, d_l, d_l, slots, 1, stride, stride, false, st); break;
-        case NTT_B200_HOST_INVERSE: run_ntt(c, d_l, d_l, slots, 1, stride, stride, true, st); break;
-        case NTT_B200_HOST_POINTWISE: launch_pointwise(c, d_l, d_l, d_r, slots, st); break;
-        default:  // the ring product: forward both, pointwise, inverse
-          run_ntt(c, d_l, d_l, slots, 1, stride, stride, false, st);
-          run_ntt(c, d_r, d_r, slots, 1, stride, stride, false, st);
-          launch_pointwise(c, d_l, d_l, d_r, slots, st);
-          run_ntt(c, d_l, d_l, slots, 1, stride, stride, true, st);
-          break;
-      }
-      CUDA_CHECK(cudaEventRecord(c.ev_comp[sl], st));
-      CUDA_CHECK(cudaStreamWaitEvent(c.copy_out, c.ev_comp[sl], 0));
-      CUDA_CHECK(cudaMemcpyAsync(values + first * n, d_l, r * n * sizeof(u64), cudaMemcpyDeviceToHost, c.copy_out));
-      CUDA_CHECK(cudaEventRecord(c.ev_out[sl], c.copy_out));
+        CUDA_CHECK(cudaMemcpyAsync(d_r + first * n, right + first * n, r * n * sizeof(u64),
+                                   cudaMemcpyHostToDevice, c.copy_in));
     }
-    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[0], 0));
-    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_out[1], 0));
+    if (!ok) {
+      // The copies already started read the caller's arrays: finish them
+      // before returning, so the caller may release the arrays at once.
+      CUDA_CHECK(cudaStreamSynchronize(c.copy_in));
+      throw ContractError("host values must be canonical residues of their towers");
+    }
+    CUDA_CHECK(cudaEventRecord(c.ev_in[0], c.copy_in));
+    CUDA_CHECK(cudaStreamWaitEvent(st, c.ev_in[0], 0));
+    std::vector<Slot> slots;
+    for (size_t i = 0; i < towers; ++i) slots.push_back({(uint32_t)i, ids[i]});
+    const u64 stride = towers * n;
+    switch (op) {
+      case NTT_B200_HOST_FORWARD: run_ntt(c, d_l, d_l, slots, 1, stride, stride, false, st); break;
+      case NTT_B200_HOST_INVERSE: run_ntt(c, d_l, d_l, slots, 1, stride, stride, true, st); break;
+      case NTT_B200_HOST_POINTWISE: launch_pointwise(c, d_l, d_l, d_r, slots, st); break;
+      default:  // the ring product: forward both, pointwise, inverse
+        run_ntt(c, d_l, d_l, slots, 1, stride, stride, false, st);
+        run_ntt(c, d_r, d_r, slots, 1, stride, stride, false, st);
+        launch_pointwise(c, d_l, d_l, d_r, slots, st);
+        run_ntt(c, d_l, d_l, slots, 1, stride, stride, true, st);
+        break;
+    }
+    CUDA_CHECK(cudaMemcpyAsync(values, d_l, towers * n * sizeof(u64), cudaMemcpyDeviceToHost, st));
     CUDA_CHECK(cudaStreamSynchronize(st));  // synchronous, as the reference's public calls are
   });
 }

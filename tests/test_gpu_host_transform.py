@@ -69,3 +69,55 @@ def test_host_validation_before_enqueue(lib, orc):
     with pytest.raises(nb.ContractError):
         g.host_transform(nb.HOST_MULTIPLY, orc.lcg(ctx.n, ctx.q[:5], 42), ids, ws)  # no right operand
     g.close()
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 128])
+def test_checks_overlap_copies_and_fail_late(lib, orc, chunk):
+    """The arrays are checked in chunks of 1, 3 or all towers while the checked
+    chunks are copied in: the results do not depend on the chunk size. A
+    non-canonical word in the last tower of the left or the right operand stops
+    the call after copies have started; both arrays are unchanged, and the next
+    call is exact."""
+    ctx = synthetic_context(orc, 4096, 7, 2, 2)
+    g = nb.Context.from_oracle(ctx)
+    ids = list(range(7))
+    mods, psis = ctx.q[:7], ctx.q_psi[:7]
+    a, b = orc.lcg(ctx.n, mods, 51), orc.lcg(ctx.n, mods, 52)
+    before = nb.tuning_get("host_chunk_towers")
+    nb.tuning_set("host_chunk_towers", chunk)
+    try:
+        ws = g.host_transform_workspace(nb.HOST_MULTIPLY)
+        for side in ("left", "right"):
+            v, r = a.copy(), b.copy()
+            (v if side == "left" else r)[6, ctx.n - 1] = mods[6]
+            keep_v, keep_r = v.copy(), r.copy()
+            with pytest.raises(nb.ContractError, match="canonical"):
+                g.host_transform(nb.HOST_MULTIPLY, v, ids, ws, right=r)
+            np.testing.assert_array_equal(v, keep_v)
+            np.testing.assert_array_equal(r, keep_r)
+        v = a.copy()
+        g.host_transform(nb.HOST_MULTIPLY, v, ids, ws, right=b)
+        np.testing.assert_array_equal(v, _ring_product(orc, mods, psis, a, b))
+    finally:
+        nb.tuning_set("host_chunk_towers", before)
+    g.close()
+
+
+def test_repeated_tower_ids_need_a_larger_workspace(lib, orc):
+    """A call may name a tower more than once; its workspace then has to hold
+    every tower of the call, more than the context's own towers."""
+    import torch
+    ctx = synthetic_context(orc, 4096, 7, 2, 2)  # 9 towers
+    g = nb.Context.from_oracle(ctx)
+    ids = [0, 1, 2, 3, 4, 5, 6, 0, 1, 2, 3]
+    mods = [ctx.q[i] for i in ids]
+    psis = [ctx.q_psi[i] for i in ids]
+    x = orc.lcg(ctx.n, mods, 53)
+    ws = g.host_transform_workspace(nb.HOST_FORWARD)
+    with pytest.raises(nb.WorkspaceError):
+        g.host_transform(nb.HOST_FORWARD, x.copy(), ids, ws)
+    big = torch.empty(len(ids) * ctx.n, dtype=torch.int64, device="cuda:0")
+    v = x.copy()
+    g.host_transform(nb.HOST_FORWARD, v, ids, big)
+    np.testing.assert_array_equal(v, orc.ntt(x, mods, psis))
+    g.close()
