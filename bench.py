@@ -839,6 +839,10 @@ def run_ours(args, rank, world, local):
     line["plain_keyswitch_per_s"] = plain["value"]
     line["plain_p50_ms"], line["plain_p99_ms"] = plain["latency_p50_ms"], plain["latency_p99_ms"]
     line["configs"] = config_legs(nb, device, *peaks())
+    # the metric's "NTT HBM GB/s": config 2 (8 x 32 towers forward + inverse, CUDA-graph replay), 2W per
+    # tower-transform, and its fraction of the HBM peak the line uses
+    c2 = line["configs"]["config2"]["graph_replay"]
+    line["ntt_hbm_gbs"], line["ntt_hbm_frac"] = c2["gb_s"], c2["frac_of_hbm_peak"]
     if not args.no_serving:
         line["serving"] = serving_legs(nb, device, value, plain["value"])
         # the metric's "served vs plain, p50/p99" at its own shape: the 0.9 x batched-capacity arrival rate
