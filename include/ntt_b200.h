@@ -468,7 +468,8 @@ int ntt_b200_setup_operations(size_t *count);
 /* Opt-in per-kernel timing: while enabled, every launch of this library is
  * bracketed by CUDA events on its own stream. query() waits for the recorded
  * events and returns the launch count and summed device time of one kernel
- * class ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col",
+ * class ("ntt_fwd_col", "ntt_fwd_row", "ntt_fwd_cluster" (a one-pass forward
+ * transform over a thread-block cluster), "ntt_inv_row", "ntt_inv_col",
  * "ntt_small", "conv", "mac", "row_mac" (the digits' forward row pass fused
  * with the key multiplication), "rotate", "correct", "pointwise", "table"). The external
  * clock protocol mirrors the reference's collect_elapsed

@@ -556,8 +556,8 @@ class KeyCache:
             pass
 
 
-KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_inv_row", "ntt_inv_col", "ntt_small", "conv", "mac",
-                  "row_mac", "rotate", "correct", "pointwise", "table")
+KERNEL_CLASSES = ("ntt_fwd_col", "ntt_fwd_row", "ntt_fwd_cluster", "ntt_inv_row", "ntt_inv_col", "ntt_small",
+                  "conv", "mac", "row_mac", "rotate", "correct", "pointwise", "table")
 
 
 def arith_probe(op: int, queries, device: int = 0):

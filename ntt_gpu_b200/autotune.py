@@ -97,6 +97,7 @@ def run(out_path: str = TUNING, iters: int = 10) -> dict:
         ("digits_lazy", (0, 1), ks_step, ("ntt_fwd_row", "mac"), unfused_mac),
         ("ntt_stage_tw_fwd_row", (0, 1), ntt_step, ("ntt_fwd_row",), {}),
         ("ntt_stage_tw_inv_row", (0, 1), ntt_step, ("ntt_inv_row",), {}),
+        ("ntt_cluster", (0, 1), ntt_step, ("ntt_fwd_col", "ntt_fwd_row", "ntt_fwd_cluster"), {}),
         ("conv_limbs", (0, 1), ks_step, ("conv",), cuda_core_conv),
         ("conv_blocks_per_sm", (4, 8, 16), ks_step, ("conv",), cuda_core_conv),
         ("mac_limbs", (0, 1), ks_step, ("mac",), unfused_mac),

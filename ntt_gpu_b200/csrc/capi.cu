@@ -489,6 +489,7 @@ Tunable g_tuning[] = {
     {"row_mac_max_beta", {4}, 1, 4},   // largest digit count the fused row pass takes (shared memory per CTA grows with it)
     {"row_mac_inv_rows", {1}, 0, 1},   // its P towers run the ModDown's inverse row pass before they are stored
     {"host_chunk_towers", {4}, 1, 128}, // towers the host-array transforms check and copy per step
+    {"ntt_cluster", {0}, 0, 1},        // plain N = 2^16 forward transforms in one pass over an 8-CTA cluster
 };
 Tunable *find_tunable(const char *name) {
   for (auto &t : g_tuning)
@@ -560,6 +561,23 @@ void launch_ntt_2pass(const Ctx &c, const b200::NttBatch &b, const NttFinal *fin
       b200::ntt_##kernel<LOGN, MODE, 4, ##__VA_ARGS__><<<grid, b200::kNttThreads, 0, st>>>(batch, c.tables); \
   } while (0)
   if (!inverse) {
+    if constexpr (LOGN == 16 && MODE == 2) {
+      // A plain forward transform (canonical outputs, no ModDown epilogue)
+      // in one pass over a thread-block cluster per tower (ntt_fwd_cluster16).
+      if (!fin && !col_only && !b.lazy_out && tuned("ntt_cluster")) {
+        static int attr_set[64] = {};
+        if (!attr_set[c.device]) {
+          CUDA_CHECK(cudaFuncSetAttribute(b200::ntt_fwd_cluster16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          b200::kClusterSmemBytes));
+          attr_set[c.device] = 1;
+        }
+        Timed t("ntt_fwd_cluster", st);
+        b200::ntt_fwd_cluster16<<<dim3(b200::kClusterCtas, polys, slots), b200::kClusterThreads,
+                                   b200::kClusterSmemBytes, st>>>(b, c.tables);
+        t.done();
+        return;
+      }
+    }
     Timed t1("ntt_fwd_col", st);
     if (tuned("ntt_col_direct"))
       NTT_LAUNCH(fwd_col, b, true);

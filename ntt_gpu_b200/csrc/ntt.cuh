@@ -19,6 +19,7 @@
 // = row pass then column pass with N^-1 folded into its last butterfly.
 // Small transforms (N <= 2048) run one CTA per tower entirely in shared memory.
 #pragma once
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "arith.cuh"
@@ -679,6 +680,134 @@ __global__ void __launch_bounds__(kNttThreads, MINB) ntt_fwd_row(NttBatch b, Dev
     fwd_row_body<LOGN, MODE, STW, DIRECT, EPI_SMEM, MODE == 2>(b, T, tile, epi_rows);
   else
     fwd_row_body<LOGN, MODE, STW, DIRECT, EPI_SMEM, false>(b, T, tile, epi_rows);
+}
+
+// ---- single-pass forward transform over a thread-block cluster (N = 2^16) -------
+// One cluster of 8 CTAs (512 threads each) per tower and polynomial; CTA k of
+// the cluster:
+//   1. runs the column pass (stages 0..7) on columns 32k .. 32k + 31, reading
+//      its inputs from global memory, and keeps the results in its shared
+//      memory as [256 rows][32 columns];
+//   2. after a cluster barrier, gathers rows 32k .. 32k + 31 (word e * 16 + u
+//      of a row lies in CTA e / 2, column (e % 2) * 16 + u) from the 8 CTAs'
+//      shared memory into registers;
+//   3. after a second barrier (every CTA has read what it needs from the
+//      others, so its shared memory is free), runs the row pass (stages
+//      8..15) on its 32 rows and stores them.
+// The tower crosses HBM once each way (2W) instead of twice (4W). Every thread
+// of every CTA of a cluster takes the same path to both barriers (the tower,
+// and so the butterflies, are the same for the whole cluster).
+constexpr int kClusterCtas = 8, kClusterThreads = 512;
+constexpr int kClusterSmemBytes = 32 * kRowPad * int(sizeof(u64));  // 32 padded rows >= 256 x 32 words
+
+template <int MODE, bool FREE>
+__device__ __forceinline__ void fwd_cluster_body(const NttBatch &b, const DeviceTables &T, u64 *sm, ulonglong2 *tw) {
+  namespace cg = cooperative_groups;
+  constexpr int LR = 8;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int k = int(cluster.block_rank());
+  const TowerView v = tower_view(b, T, false);
+  const u64 q = v.c->q, q2 = v.c->q2;
+  u64 x[16];
+  {
+    // Column pass: thread (c, u), column 32k + c; mapping A holds rows
+    // e * 16 + u (stages 0..3), mapping B rows u * 16 + e (stages 4..7).
+    const int c = threadIdx.x % 32, u = threadIdx.x / 32;
+    const u64 *in = v.src + 32 * k + c;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = in[(e * 16 + u) * 256];
+    for (int i = threadIdx.x; i < 256; i += kClusterThreads) tw[i] = v.tw[i];
+    __syncthreads();
+#pragma unroll
+    for (int st = 0; st < 4; ++st) {
+      const int d = 8 >> st;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const ulonglong2 w = tw[(1 << st) + (e >> (4 - st))];
+        if (st == 0)
+          ct_bf<FREE, MODE, true>(x[e], x[e + d], w.x, w.y, q, q2);
+        else
+          ct_bf<FREE, MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) sm[(e * 16 + u) * 32 + c] = x[e];
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 16; ++e) x[e] = sm[(u * 16 + e) * 32 + c];
+#pragma unroll
+    for (int st = 4; st < LR; ++st) {
+      const int d = 1 << (LR - 1 - st);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e & d) continue;
+        const ulonglong2 w = tw[(1 << st) + ((u * 16 + e) >> (LR - st))];
+        ct_bf<FREE, MODE>(x[e], x[e + d], w.x, w.y, q, q2);
+      }
+    }
+    // Each word of mapping B is read and rewritten by the same thread.
+#pragma unroll
+    for (int e = 0; e < 16; ++e) sm[(u * 16 + e) * 32 + c] = x[e];
+  }
+  cluster.sync();  // every CTA's column results are complete and visible to the cluster
+  // Row pass: thread (r, u), row 32k + r; warp w owns rows 2w and 2w + 1.
+  const int r = threadIdx.x / 16, u = threadIdx.x % 16;
+  const int row = 32 * k + r;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const u64 *owner = cluster.map_shared_rank(sm, unsigned(e >> 1));
+    x[e] = owner[row * 32 + (e & 1) * 16 + u];
+  }
+  cluster.sync();  // every CTA has read its rows from the others: shared memory is free
+  u64 *my = sm + r * kRowPad;
+#pragma unroll
+  for (int sp = 0; sp < 4; ++sp) {
+    const int st = LR + sp, d = 8 >> sp;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(v.tw + (1 << st) + (row << sp) + (e >> (4 - sp)));
+      ct_bf<FREE, MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) my[pad_col(e * 16 + u)] = x[e];
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < 16; ++e) x[e] = my[pad_col(u * 16 + e)];
+#pragma unroll
+  for (int sp = 4; sp < 8; ++sp) {
+    const int st = LR + sp, d = 1 << (7 - sp);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      const Shoup w = tw_load(v.tw + (1 << st) + (row << sp) + row_lane_major(u, e >> (8 - sp)));
+      ct_bf<FREE, MODE>(x[e], x[e + d], w.w, w.wq, q, q2);
+    }
+  }
+  const u64 one = v.c->red.one;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    if constexpr (FREE)
+      x[e] = reduce_free_final(x[e], q, one);
+    else
+      x[e] = reduce_final<MODE>(x[e], q, q2);
+    my[pad_col(u * 16 + e)] = x[e];
+  }
+  __syncwarp();
+  store_rows_warp(tower_dst(b, T, fresh_block_ids()) + u64(32 * k) * 256, sm);
+}
+
+// The cluster's tower decides the butterflies: reduction-free below 2^57.
+static __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kClusterThreads, 2)
+    ntt_fwd_cluster16(NttBatch b, DeviceTables T) {
+  extern __shared__ __align__(16) u64 sm[];
+  __shared__ ulonglong2 tw[256];
+  if (T.tc[b.id[blockIdx.z]].q < kFreeModulusBound)
+    fwd_cluster_body<2, true>(b, T, sm, tw);
+  else
+    fwd_cluster_body<2, false>(b, T, sm, tw);
 }
 
 // The inverse row pass's butterflies (stages logR + 7 .. logR, Gentleman-Sande)

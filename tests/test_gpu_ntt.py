@@ -132,3 +132,43 @@ def test_butterfly_mode_boundaries(lib, orc, bits, logn):
         np.testing.assert_array_equal(nb.to_host(back), x)
         ctx.ntt(out, nb.to_device(x), ids, inverse=True)
         np.testing.assert_array_equal(nb.to_host(out), orc.ntt(x, q, psi, inverse=True))
+
+
+@pytest.mark.parametrize("inplace", [False, True])
+def test_cluster_forward_transform(lib, orc, inplace):
+    """The one-pass forward transform over an 8-CTA cluster (ntt_cluster, N = 2^16:
+    column pass, rows gathered through distributed shared memory, row pass) on
+    3 polynomials of 50-, 55- and 60-bit towers (reduction-free and per-stage
+    reducing butterflies in one launch) and all-(q-1) inputs, in and out of
+    place: equal to the oracle and to the two-pass transform. The host-array
+    forward call takes the same path."""
+    n, polys = 1 << 16, 3
+    q, psi = towers_for(orc, n, [50, 55, 60, 50, 60])
+    q += primes_below(orc, n, 1, 1 << 57)
+    psi = [orc.find_psi(v, n) for v in q]
+    ctx = nb.Context(n, q, psi)
+    ids = list(range(len(q)))
+    xs = [orc.lcg(n, q, 300 + p) for p in range(polys - 1)]
+    xs.append(np.array([[v - 1] * n for v in q], dtype=np.uint64))
+    x = np.stack(xs)
+    stride = len(q) * n
+    got = {}
+    before = nb.tuning_get("ntt_cluster")
+    try:
+        for cluster in (1, 0):
+            nb.tuning_set("ntt_cluster", cluster)
+            d = nb.to_device(x)
+            out = d if inplace else nb.empty(x.shape)
+            ctx.ntt(out, d, ids, polys=polys, poly_stride=stride)
+            got[cluster] = nb.to_host(out)
+        nb.tuning_set("ntt_cluster", 1)
+        ws = ctx.host_transform_workspace(nb.HOST_FORWARD)
+        h = x[0].copy()
+        ctx.host_transform(nb.HOST_FORWARD, h, ids, ws)
+    finally:
+        nb.tuning_set("ntt_cluster", before)
+    for p in range(polys):
+        np.testing.assert_array_equal(got[1][p], orc.ntt(x[p], q, psi), err_msg=f"poly {p}")
+    np.testing.assert_array_equal(got[1], got[0])
+    np.testing.assert_array_equal(h, got[0][0])
+    ctx.close()

@@ -17,7 +17,7 @@ VARIANTS = [("ntt_minb_fwd_col", 3), ("ntt_minb_fwd_row", 3), ("ntt_minb_inv_row
             ("intt_unscaled", 0), ("digits_lazy", 0), ("ntt_stage_tw_fwd_row", 1), ("ntt_stage_tw_inv_row", 1), ("conv_limbs", 0),
             ("conv_blocks_per_sm", 2), ("conv_tc_tiles", 3), ("conv_tc_fixed", 0), ("mac_limbs", 1),
             ("mac_approx", 0), ("mac_rotate", 0), ("conv_tc", 0), ("row_mac", 0),
-            ("row_mac_max_beta", 1), ("row_mac_inv_rows", 0)]
+            ("row_mac_max_beta", 1), ("row_mac_inv_rows", 0), ("ntt_cluster", 1)]
 
 
 def _check_paths(orc):

@@ -11,7 +11,7 @@ EXPECTED = {"ntt_minb_fwd_col", "ntt_minb_fwd_row", "ntt_minb_inv_row", "ntt_min
             "ntt_col_direct", "ntt_row_direct", "ntt_epi_stage", "intt_unscaled", "digits_lazy", "ntt_stage_tw_fwd_row",
             "ntt_stage_tw_inv_row", "conv_limbs", "conv_blocks_per_sm", "conv_tc_tiles", "conv_tc_fixed",
             "mac_limbs", "mac_approx", "mac_rotate", "conv_tc", "row_mac", "row_mac_max_beta",
-            "row_mac_inv_rows", "host_chunk_towers"}
+            "row_mac_inv_rows", "host_chunk_towers", "ntt_cluster"}
 
 
 def test_tunables_are_listed_and_range_checked():
