@@ -640,13 +640,26 @@ __device__ __forceinline__ void fwd_row_body(const NttBatch &b, const DeviceTabl
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncwarp();
   }
+  // Without STW, chunk `it` of lane l in warp w is row 2w + it / 4, columns
+  // c = 2l + 64 (it % 4): a per-thread base plus constants (pad_col(c) =
+  // 2l + l / 8 + 68 (it % 4)), so no chunk recomputes its address.
+  const int lane = threadIdx.x & 31;
+  const int gbase = int(threadIdx.x >> 5) * 512 + 2 * lane;
+  const int sbase = int(threadIdx.x >> 5) * 2 * kRowPad + 2 * lane + (lane >> 3);
 #pragma unroll
   for (int it = 0; it < 8; ++it) {
-    const int j = j0 + it * kJStep;
-    const int rr = j >> 7, c = (j & 127) * 2;
-    const int sidx = rr * kRowPad + pad_col(c);
-    const ulonglong2 l = EPI_SMEM ? *reinterpret_cast<const ulonglong2 *>(epi_rows + rr * 256 + c)
-                                  : *reinterpret_cast<const ulonglong2 *>(left + rr * 256 + c);
+    int goff, sidx;
+    if constexpr (STW) {
+      const int j = j0 + it * kJStep;
+      const int rr = j >> 7, c = (j & 127) * 2;
+      goff = rr * 256 + c;
+      sidx = rr * kRowPad + pad_col(c);
+    } else {
+      goff = gbase + (it >> 2) * 256 + 64 * (it & 3);
+      sidx = sbase + (it >> 2) * kRowPad + 68 * (it & 3);
+    }
+    const ulonglong2 l = EPI_SMEM ? *reinterpret_cast<const ulonglong2 *>(epi_rows + goff)
+                                  : *reinterpret_cast<const ulonglong2 *>(left + goff);
     ulonglong2 o;
     if constexpr (MODE == 2) {
       // left < q and x < 4q: left + 4q - x lies in (0, 5q), below 2^64 for q < 2^61;
@@ -661,11 +674,11 @@ __device__ __forceinline__ void fwd_row_body(const NttBatch &b, const DeviceTabl
       o.y = shoup_canon(sub_mod(l.y, tile[sidx + 1], q), pinv.w, pinv.wq, q);
     }
     if (add) {
-      const ulonglong2 e = *reinterpret_cast<const ulonglong2 *>(add + rr * 256 + c);
+      const ulonglong2 e = *reinterpret_cast<const ulonglong2 *>(add + goff);
       o.x = add_mod(o.x, e.x, q);
       o.y = add_mod(o.y, e.y, q);
     }
-    *reinterpret_cast<ulonglong2 *>(out + rr * 256 + c) = o;
+    *reinterpret_cast<ulonglong2 *>(out + goff) = o;
   }
 }
 
