@@ -196,11 +196,16 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
     const uint32_t gi = ROT ? inverse_mod_pow2(mb.g) : 1u;
     Shoup pm{0, 0};
     if (ROT && mb.c0 && !PT) pm = a.mac.plan->p_mod[t];
+    // Step `it` of a lane takes row wrow + it / 4, columns c = 2 lane +
+    // 64 (it % 4): a per-lane base plus offsets (pad_col(c) = 2 lane +
+    // lane / 8 + 68 (it % 4) in shared memory).
+    const u64 ibase = u64(wrow) * 256 + 2 * lane;
+    const int sbase = 2 * warp * kRowPad + 2 * lane + (lane >> 3);
 #pragma unroll 2
     for (int it = 0; it < 8; ++it) {
-      const int j = lane + 32 * it;
-      const int rr = j >> 7, c = (j & 127) * 2;
-      const u64 i = u64(wrow + rr) * 256 + c;
+      const int rr = it >> 2;
+      const u64 i = ibase + rr * 256 + 64 * (it & 3);
+      const int soff = sbase + rr * kRowPad + 68 * (it & 3);
       Acc128 b0{}, b1{}, a0{}, a1{};
 #pragma unroll
       for (int d = 0; d < BETA; ++d) {
@@ -209,7 +214,7 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
           x = *reinterpret_cast<const ulonglong2 *>(mb.input + u64(t) * N + i);
         } else {
           const int region = PT ? d : (d < own ? d : d - 1);
-          const u64 *sd = rm_digits + (region * kRows + 2 * warp + rr) * kRowPad + pad_col(c);
+          const u64 *sd = rm_digits + region * kRows * kRowPad + soff;
           x = make_ulonglong2(sd[0], sd[1]);
         }
         const ulonglong2 vb = *reinterpret_cast<const ulonglong2 *>(kb[d] + i);
@@ -227,7 +232,7 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
       if (inv_rows) {
         // Channel b over digit 0's words of these two slots, channel a over
         // digit 1's: this lane has read them above and no other lane reads them.
-        u64 *sb = rm_digits + (2 * warp + rr) * kRowPad + pad_col(c);
+        u64 *sb = rm_digits + soff;
         u64 *sa = sb + kRows * kRowPad;
         sb[0] = rb.x;
         sb[1] = rb.y;
