@@ -448,24 +448,29 @@ __device__ __forceinline__ int pad_col(int col) { return col + (col >> 4); }
 // (rows 2w and 2w+1 of the tile belong to warp w in both row passes): 16-byte
 // coalesced chunks and no CTA-wide barrier, so the warps of a CTA run their
 // load, butterfly and store phases independently and overlap one another.
+// Step `it` (0..7) of lane l copies columns c = 2l + 64 (it % 4) of row
+// 2w + it / 4: a per-lane base plus constants (pad_col(c) = 2l + l / 8 +
+// 68 (it % 4)).
 __device__ __forceinline__ void load_rows_warp(u64 *tile, const u64 *g) {
   const int lane = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 2;
+  const u64 *gb = g + r0 * 256 + 2 * lane;
+  u64 *tb = tile + r0 * kRowPad + 2 * lane + (lane >> 3);
 #pragma unroll
-  for (int j = lane; j < 256; j += 32) {
-    const int rr = r0 + (j >> 7), c = (j & 127) * 2;
-    const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(g + rr * 256 + c);
-    const int sidx = rr * kRowPad + pad_col(c);
-    tile[sidx] = v.x;
-    tile[sidx + 1] = v.y;
+  for (int it = 0; it < 8; ++it) {
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(gb + (it >> 2) * 256 + 64 * (it & 3));
+    u64 *t = tb + (it >> 2) * kRowPad + 68 * (it & 3);
+    t[0] = v.x;
+    t[1] = v.y;
   }
 }
 __device__ __forceinline__ void store_rows_warp(u64 *g, const u64 *tile) {
   const int lane = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 2;
+  u64 *gb = g + r0 * 256 + 2 * lane;
+  const u64 *tb = tile + r0 * kRowPad + 2 * lane + (lane >> 3);
 #pragma unroll
-  for (int j = lane; j < 256; j += 32) {
-    const int rr = r0 + (j >> 7), c = (j & 127) * 2;
-    const int sidx = rr * kRowPad + pad_col(c);
-    *reinterpret_cast<ulonglong2 *>(g + rr * 256 + c) = make_ulonglong2(tile[sidx], tile[sidx + 1]);
+  for (int it = 0; it < 8; ++it) {
+    const u64 *t = tb + (it >> 2) * kRowPad + 68 * (it & 3);
+    *reinterpret_cast<ulonglong2 *>(gb + (it >> 2) * 256 + 64 * (it & 3)) = make_ulonglong2(t[0], t[1]);
   }
 }
 
