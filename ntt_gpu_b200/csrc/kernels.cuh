@@ -318,10 +318,11 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(const __grid_consta
   // the previous tile's matrix products and reductions run.
   auto stage_tile = [&](uint32_t tile) {
     const u64 *rows = src + u64(tile) * kTcThreads;
-    for (int c = tid; c < s * (kTcThreads / 2); c += kTcThreads) {
-      const int j = c / (kTcThreads / 2), w = (c % (kTcThreads / 2)) * 2;
+    // Each pass of the CTA copies two source rows: row j, words w and w + 1.
+    const int w = (tid & (kTcThreads / 2 - 1)) * 2;
+#pragma unroll(FS ? 8 : 1)
+    for (int j = tid / (kTcThreads / 2); j < s; j += 2)
       tc_copy16(stage + (j * kTcThreads + w) * sizeof(u64), rows + u64(j) * n + w);
-    }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   const uint32_t first = blockIdx.x * uint32_t(a.tiles_per_cta);

@@ -115,13 +115,13 @@ __device__ __forceinline__ void row_mac_body(const RowMacArgs &a, const DeviceTa
   auto stage_rows = [&](int i) {
     uint32_t ln = lane;
     asm volatile("" : "+r"(ln));
-    const u64 *src = a.digits + input * a.digit_stride + (u64(digit_of(i)) * a.towers + t) * N + u64(wrow) * 256;
-    u64 *dst = rm_digits + (i * kRows + 2 * warp) * kRowPad;
+    // Word k of the lane: row k / 8 of the warp's two, column ln + 32 (k % 8)
+    // (pad_col of it: ln + ln / 16 + 34 (k % 8)).
+    const u64 *src =
+        a.digits + input * a.digit_stride + (u64(digit_of(i)) * a.towers + t) * N + u64(wrow) * 256 + ln;
+    u64 *dst = rm_digits + (i * kRows + 2 * warp) * kRowPad + ln + (ln >> 4);
 #pragma unroll 4
-    for (int k = 0; k < 16; ++k) {
-      const int j = int(ln) + 32 * k, rr = j >> 8, c = j & 255;
-      rm_copy8(dst + rr * kRowPad + pad_col(c), src + rr * 256 + c);
-    }
+    for (int k = 0; k < 16; ++k) rm_copy8(dst + (k >> 3) * kRowPad + 34 * (k & 7), src + (k >> 3) * 256 + 32 * (k & 7));
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   if constexpr (kMaxRegions > 0) stage_rows(0);
