@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(const __grid_consta
     const int w = (tid & (kTcThreads / 2 - 1)) * 2;
 #pragma unroll(FS ? 8 : 1)
     for (int j = tid / (kTcThreads / 2); j < s; j += 2)
-      tc_copy16(stage + (j * kTcThreads + w) * sizeof(u64), rows + u64(j) * n + w);
+      tc_copy16(stage + (j * kTcThreads + w) * sizeof(u64), rows + (u64(j) << a.logn) + w);
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   const uint32_t first = blockIdx.x * uint32_t(a.tiles_per_cta);
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(kTcThreads) conv_tc_kernel(const __grid_consta
           const u64 m = tm[t];
           u64 r = tc_fold_reduce(hi4, lo4, 0 - m, twq[t]);  // [0, 3.5m)
           if constexpr (!LAZY_OUT) r = csub_sign(csub_sign(r, 2 * m), m);
-          dst[u64(part.slot[t]) * n + k] = r;
+          dst[(u64(part.slot[t]) << a.logn) + k] = r;  // slot * n (n = 2^logn)
         }
       }
       // Every lane's loads are done before the next MMA reuses the columns.
