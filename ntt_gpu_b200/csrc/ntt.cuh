@@ -274,14 +274,17 @@ __device__ __forceinline__ void fwd_col_body(const NttBatch &b, const DeviceTabl
     __syncthreads();
 #pragma unroll
     for (int e = 0; e < 16; ++e) x[e] = tile[G::row_b(e, u) * G::COLS + c];
-    // Stages 4..logR-1: row bit logR-1-s == register bit logR-1-s.
+    // Stages 4..logR-1: row bit logR-1-s == register bit logR-1-s. With
+    // row_b(e, u) = 16u + e and k = logR - s <= 4 the twiddle is entry
+    // (1 << s) + (u << (4 - k)) + (e >> k): one base per stage.
 #pragma unroll
     for (int s = 4; s < G::LR; ++s) {
-      const int d = 1 << (G::LR - 1 - s);
+      const int d = 1 << (G::LR - 1 - s), k = G::LR - s;
+      const ulonglong2 *tws = tw + (1 << s) + (u << (4 - k));
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         if (e & d) continue;
-        const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+        const ulonglong2 w = tws[e >> k];
         ct_bf<FREE, MODE>(x[e], x[e + d], w.x, w.y, q, q2);
       }
     }
@@ -351,19 +354,20 @@ __device__ __forceinline__ void inv_col_body(const NttBatch &b, const DeviceTabl
       gs_stages_light<4, G::LR - 4>(
           x,
           [&](int j, int e) {
-            const int s = G::LR - 1 - j;
-            const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+            const int s = G::LR - 1 - j, k = G::LR - s;  // row_b(e, u) >> k = (u << (4 - k)) + (e >> k)
+            const ulonglong2 w = tw[(1 << s) + (u << (4 - k)) + (e >> k)];
             return Shoup{w.x, w.y};
           },
           q);
     } else {
 #pragma unroll
       for (int s = G::LR - 1; s >= 4; --s) {
-        const int d = 1 << (G::LR - 1 - s);
+        const int d = 1 << (G::LR - 1 - s), k = G::LR - s;
+        const ulonglong2 *tws = tw + (1 << s) + (u << (4 - k));  // as in the forward pass
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
           if (e & d) continue;
-          const ulonglong2 w = tw[(1 << s) + (G::row_b(e, u) >> (G::LR - s))];
+          const ulonglong2 w = tws[e >> k];
           gs_butterfly<MODE>(x[e], x[e + d], w.x, w.y, q, q2);
         }
       }
