@@ -1307,7 +1307,9 @@ std::vector<Chunk> plan_chunks(const ntt_b200_ks_request *reqs, size_t count) {
 
 // Words of a chunk's device table: ReqDesc[r] | usrc[u] | dst_list[2r] |
 // add_list[2r] | groups[u] (input u's requests: first | count << 32).
-size_t table_words(size_t r, size_t u) { return 6 * r + u + 4 * r + u; }
+constexpr size_t table_words(size_t r, size_t u) { return 6 * r + u + 4 * r + u; }
+// A full chunk (every request with its own input) fits put_table's largest form.
+static_assert(table_words(kMaxGroup, kMaxGroup) <= 2048, "request table of a full chunk exceeds put_words");
 
 size_t chunk_bytes(const Ctx &c, const Chunk &ch) {
   const size_t n = c.n, L = ch.level, K = c.k, T = L + K, r = ch.idx.size(), u = ch.usrc.size();
