@@ -146,6 +146,31 @@ __host__ __device__ constexpr int gs_bound(int f, int e, int j) {
     if ((e >> i) & 1) last = i;
   return last < 0 ? f << j : 4 << (j - 1 - last);
 }
+// Compile-time proof of gs_bound for F and STAGES, by the stage-by-stage
+// propagation it summarises: bounds in units of q, registers entering below F;
+// in each pair the sum's bound is the sum of both, the difference side leaves
+// the product below 4. It also checks what the butterflies rely on: both
+// registers of a pair share a bound B (so x + Bq - y never underflows), the
+// product's input x + Bq - y < 2Bq and every bound stay at or below 64
+// (64q < 2^63 for q < 2^57: no wrap, and csub_sign's sign test holds), and
+// the halving ladder at the end (32q, 16q, 8q, 4q) reaches 4q from any bound
+// up to 64.
+__host__ __device__ constexpr bool gs_bound_holds(int f, int stages) {
+  int b[16] = {};
+  for (int e = 0; e < 16; ++e) b[e] = f;
+  for (int j = 0; j < stages; ++j) {
+    const int d = 1 << j;
+    for (int e = 0; e < 16; ++e) {
+      if (e & d) continue;
+      if (b[e] != gs_bound(f, e, j) || b[e + d] != b[e] || 2 * b[e] > 64) return false;
+      b[e] += b[e + d];
+      b[e + d] = 4;
+    }
+  }
+  for (int e = 0; e < 16; ++e)
+    if (b[e] != gs_bound(f, e, stages) || b[e] > 64) return false;
+  return true;
+}
 template <int F, int STAGES, typename TwOf>
 __device__ __forceinline__ void gs_stages_light(u64 (&x)[16], TwOf tw_of, u64 q) {
   const u64 qneg = 0 - q;
@@ -162,6 +187,7 @@ __device__ __forceinline__ void gs_stages_light(u64 (&x)[16], TwOf tw_of, u64 q)
     }
   }
   static_assert(F <= 4 && STAGES <= 4, "bounds stay at or below 64q");
+  static_assert(gs_bound_holds(F, STAGES), "gs_bound disagrees with the stage-by-stage bounds");
   const u64 q4 = 4 * q, q8 = 8 * q, q16 = 16 * q, q32 = 32 * q;
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
