@@ -97,12 +97,17 @@ __device__ __forceinline__ void ct_butterfly(u64 &x, u64 &y, u64 w, u64 wq, u64 
 //   x' = x + t, y' = x + 4q - t,
 // so from inputs in [0, R) both outputs lie in [0, R + 4q): the range grows by
 // 4q per stage. A forward transform starts below 4q and runs at most 16
-// stages, so every value stays below 68q < 2^63 for q < 2^57, and the
-// products accept any 64-bit input. The per-stage conditional subtraction of
+// stages, so every value stays below 68q < 2^64 for q < 2^57 (not always
+// below 2^63: 68q passes 2^63 once q > 2^63 / 68). Nothing needs the top bit
+// clear: the products accept any 64-bit input, the consumers below reduce
+// with reduce64_approx (any word) before any conditional subtraction, and the
+// ModDown epilogue's left + 68q - x stays below 69q < 2^64. The per-stage conditional subtraction of
 // ct_butterfly (most of its ALU work) disappears; the transform's consumer
 // reduces once (reduce_free_final) or takes the lazy values directly.
 constexpr u64 kFreeModulusBound = u64(1) << 57;
 constexpr int kFreeRangeFactor = 68;  // values stay below 68q
+static_assert(kFreeRangeFactor == 4 + 4 * 16, "inputs below 4q, 4q more per stage, at most 16 stages (N <= 2^16)");
+static_assert(u64(kFreeRangeFactor + 1) <= ~u64(0) / kFreeModulusBound, "69q (the epilogue's span) fits a word");
 template <bool FREE, int MODE, bool FRESH = false>
 __device__ __forceinline__ void ct_bf(u64 &x, u64 &y, u64 w, u64 wq, u64 q, u64 q2) {
   if constexpr (FREE) {
